@@ -1,0 +1,330 @@
+#!/usr/bin/env python3
+"""Benchmark of the Monte Carlo hot path on B200.
+
+Workload (one "step" = one full pricing of it): a Bates model under Andersen QE
+(psi_c = 1.5), 16,777,216 paths x 252 daily steps, FP32 stepping with FP64
+accumulation, five payoffs priced in one pass (European call K=100, arithmetic
+Asian call K=100, up-and-out call K=100 B=130 daily monitoring, floating-strike
+lookback put, cash-or-nothing binary call K=105 paying 1); S0=100, T=1, r=0.03,
+q=0, v0=0.04, kappa=2, theta=0.04, sigma=0.3, rho=-0.7, lambda=0.1, muJ=-0.05,
+sigmaJ=0.10.  Synthetic: the inputs are these parameters; paths come from Philox.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 launch with torchrun (one process per GPU); every rank prices its own
+contract on its own Philox stream (weak scaling, no data-path collective); the
+timed region is bracketed by a barrier and device syncs and the max over ranks is
+reported.  Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_PATHS = 16_777_216
+N_STEPS = 252
+WORKLOAD = "bates_qe_5payoff_16777216x252_fp32"
+METRIC = "path-steps/s"
+# Algorithmic per-path-step work of the fused Bates-QE kernel, counted from the step
+# formulas (not from SASS): 13 SFU ops (4 Box-Muller: lg2, rsqrt, sin, cos; 9 QE:
+# rcp m, rcp psi, rsqrt, rcp(1+b2), rsqrt b2, rcp term, lg2 term, rsqrt, ex2) and
+# 131 issued instructions (Philox4x32-10 ~66, Box-Muller ~14, QE step ~38,
+# Poisson test + tracking + loop ~13).
+SFU_PER_STEP = 13.0
+ISSUE_PER_STEP = 131.0
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-sample-paths", type=int, default=1 << 16)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
+    return ap.parse_args()
+
+
+def workload_contract(qk, rank: int = 0, precision=None, n_paths: int = N_PATHS):
+    legs = [qk.payoff(qk.EUROPEAN, qk.CALL, 100.0), qk.payoff(qk.ASIAN, qk.CALL, 100.0),
+            qk.payoff(qk.BARRIER_UP_OUT, qk.CALL, 100.0, 130.0), qk.payoff(qk.LOOKBACK_FLOATING, qk.PUT, 100.0),
+            qk.payoff(qk.BINARY_CASH, qk.CALL, 105.0)]
+    return qk.make_contract(S0=100.0, v0=0.04, r=0.03, q=0.0, model=qk.BATES, scheme=qk.ANDERSEN_QE, kappa=2.0,
+                            theta=0.04, sigma=0.3, rho=-0.7, lambda_j=0.1, mu_j=-0.05, sigma_j=0.10, psi_c=1.5,
+                            T=1.0, n_steps=N_STEPS, n_paths=n_paths, seed=42, stream=rank,
+                            precision=qk.FP32 if precision is None else precision, payoffs=legs)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="qk_clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, max_mhz_hint: float) -> dict:
+        rows = []
+        try:
+            for line in self.path.read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": max_mhz_hint, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()) if rows else None}
+
+
+# ----------------------------------------------------------------------------- CPU / reference leg
+def cpu_reference_rate(sample_paths: int, repeats: int = 1) -> dict:
+    """The reference's own pricing path on the host cores (oracle/_ref: reference headers over the
+    OpenMP host shim), one run per payoff leg as the reference prices one payoff per run; falls back
+    to the C restatement (oracle/qk_oracle.c, all legs in one pass) when the reference was not built."""
+    from oracle import qkref
+    cores = os.cpu_count() or 1
+    legs = [(0, 0, 100.0, 100.0), (1, 0, 100.0, 100.0), (2, 0, 100.0, 130.0), (6, 1, 100.0, 100.0),
+            (8, 0, 105.0, 100.0)]
+    if qkref.available():
+        total = 0.0
+        for _ in range(repeats):
+            for t, r, K, B in legs:
+                cfg = qkref.config(S0=100.0, v0=0.04, r=0.03, q=0.0, opt_type=t, opt_right=r, K=K, B=B, model=1,
+                                   scheme=2, kappa=2.0, theta=0.04, sigma=0.3, rho=-0.7, lambda_j=0.1, mu_j=-0.05,
+                                   sigma_j=0.10, T=1.0, dt_in=1.0 / N_STEPS, n_paths=sample_paths, seed=42,
+                                   max_cpu_ram_mb=64000)
+                t0 = time.perf_counter()
+                qkref.price(cfg, 8)
+                total += time.perf_counter() - t0
+        kind = "reference"
+        sample = (f"{sample_paths} paths x {N_STEPS} steps, 5 reference runs (one per payoff leg, FP64, "
+                  f"OpenMP over the host shim)")
+    else:
+        import quantkos_b200 as qk
+        from oracle import qkoracle
+        k = workload_contract(qk, 0, qk.FP64, sample_paths)
+        t0 = time.perf_counter()
+        for _ in range(repeats):
+            qkoracle.price(k)
+        total = time.perf_counter() - t0
+        kind = "port"
+        sample = f"{sample_paths} paths x {N_STEPS} steps, C restatement, all legs in one pass, FP64"
+    value = repeats * sample_paths * N_STEPS / total
+    return {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample, "seconds": total}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_reference_rate(args.cpu_sample_paths)
+    r = cpu_reference_rate(args.cpu_sample_paths, repeats=args.steps)
+    ms_per_step = 1e3 * r["seconds"] / args.steps
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_paths": args.cpu_sample_paths, "n_steps": N_STEPS,
+                       "note": "bounded sample of the workload per step"},
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def main() -> None:
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import quantkos_b200 as qk
+
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    h = qk.Handle(local_rank)
+    ext = torch.cuda.ExternalStream(h.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    contract = workload_contract(qk, rank)
+    path_steps = float(N_PATHS) * N_STEPS
+
+    # ---- value: descriptors resident in HBM, K device-timed pricings
+    prep = qk.PreparedBatch([contract], None, h)
+    for _ in range(max(args.warmup, 3)):
+        prep.run()
+        prep.fetch()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms, launches = [], 0
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        for i in range(args.steps):
+            flush.fill_(float(i))  # L2 flush (256 MiB > 126 MB L2) outside the timed events
+            torch.cuda.synchronize()
+            starts[i].record(ext)
+            prep.run()
+            ends[i].record(ext)
+            res = prep.fetch()
+            t = h.last_timing()
+            kernel_ms.append(t["paths_ms"])
+            launches += t["launches"]
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = max_over_ranks(sum(step_ms))
+    ms_per_step = total_ms / args.steps
+    value = world * path_steps / (ms_per_step * 1e-3)
+
+    # ---- e2e: the public call with host buffers (plan + H2D descriptors + kernels + D2H results)
+    for _ in range(2):
+        qk.price_batch([contract], None, h)
+    e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    barrier()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        e_s[i].record(ext)
+        qk.price_batch([contract], None, h)
+        e_e[i].record(ext)
+        t = h.last_timing()
+        h2d, d2h = t["h2d_bytes"], t["d2h_bytes"]
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_s, e_e))) / args.steps
+    e2e_value = world * path_steps / (e2e_ms * 1e-3)
+
+    # ---- roofline of the dominant kernel (the fused path kernel)
+    sfu_ops = h.measure_sfu()
+    peak_ps = sfu_ops / max(SFU_PER_STEP, ISSUE_PER_STEP / 8.0)  # issue rate = 8 x SFU rate (128 vs 16 lanes/clk/SM)
+    kern_ms = statistics.mean(kernel_ms)
+    achieved_ps = path_steps / (kern_ms * 1e-3)
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            tj = json.loads(tf.read_text())
+            traffic = tj["dram_bytes_per_path_step"] * path_steps
+        except (ValueError, KeyError):
+            traffic = None
+
+    # ---- plain FP64 drop-in on the same workload (equal paths => equal standard error)
+    plain = None
+    if not args.no_plain:
+        c64 = workload_contract(qk, rank, qk.FP64)
+        qk.price_plain(c64, None, h)
+        r64 = qk.price_plain(c64, None, h)
+        t64 = h.last_timing()
+        plain = {"ms": t64["device_ms"], "value": path_steps / (t64["device_ms"] * 1e-3),
+                 "speedup_of_value": value / world / (path_steps / (t64["device_ms"] * 1e-3)),
+                 "std_error_fp64": [leg["std_error"] for leg in r64["legs"]],
+                 "std_error_fp32": [leg["std_error"] for leg in res[0]["legs"]],
+                 "price_fp64": [leg["price"] for leg in r64["legs"]],
+                 "price_fp32": [leg["price"] for leg in res[0]["legs"]]}
+
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    clocks = sampler.summary(peaks.get("sm_max_mhz", 1965.0))
+
+    cpu = None
+    if rank == 0 and world == 1:
+        try:
+            cpu = {k: v for k, v in cpu_reference_rate(args.cpu_sample_paths).items() if k != "seconds"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable", "sample": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_paths": N_PATHS, "n_steps": N_STEPS, "payoff_legs": 5,
+                       "parallelism": f"contract-per-gpu x{world}", "l2": "flushed between timed steps (256 MiB write)",
+                       "contracts_per_s": world / (ms_per_step * 1e-3)},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_ms},
+            "roofline": {"bound": "sfu", "achieved": achieved_ps / 1e9, "peak": peak_ps / 1e9,
+                         "unit": "Gpath-steps/s", "frac": achieved_ps / peak_ps, "traffic": traffic,
+                         "kernel": "price_tiles_kernel<float>", "kernel_ms": kern_ms,
+                         "peak_source": f"measured SFU rate {sfu_ops / 1e12:.3f} Tops/s (qk_measure_sfu); "
+                                        f"per path-step {SFU_PER_STEP:.0f} SFU / {ISSUE_PER_STEP:.0f} issued"},
+            "cpu_baseline": cpu,
+            "plain_fp64": plain,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    h.close()
+
+
+if __name__ == "__main__":
+    main()

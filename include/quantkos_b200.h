@@ -1,0 +1,273 @@
+/*
+ * quantkos_b200.h — C ABI of the B200-native QuantKos Monte Carlo hot path.
+ *
+ * The reference (QuantKos) has no FFI: its boundary is a C++ template API whose
+ * pieces are named beside each entry point below (paths relative to the
+ * reference project).  This header is the drop-in boundary that replaces them:
+ * plain C types, caller-owned host arrays, handle-owned device memory, integer
+ * status codes (never abort, never trap).  The C++ wrappers with the
+ * reference's own names live in quantkos_b200.hpp; INTEGRATION.md shows the
+ * bindings a maintainer adds.
+ *
+ * Threading: a handle is used by one host thread at a time, except
+ * qk_serve_submit / qk_serve_poll, which are thread-safe.
+ */
+#ifndef QUANTKOS_B200_H
+#define QUANTKOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QK_ABI_VERSION 1
+#define QK_MAX_PAYOFFS 8
+
+/* ---------------------------------------------------------------- status */
+typedef enum qk_status {
+    QK_OK = 0,
+    QK_ERR_INVALID_ARG = 1,   /* std::invalid_argument in the reference (Config.hpp validate()) */
+    QK_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    QK_ERR_OUT_OF_MEMORY = 3, /* std::runtime_error "[Memory Capacity Error]" (PathsMCBatchMem.hpp:396-415) */
+    QK_ERR_UNSUPPORTED = 4,   /* runtime_error "not yet implemented for this scheme combination" (MSchemes.hpp:51-54) */
+    QK_ERR_TIMEOUT = 5,       /* a bounded device/host wait gave up */
+    QK_ERR_CAPACITY = 6,      /* request larger than the admission budget */
+    QK_ERR_NO_DEVICE = 7,
+    QK_ERR_PARSE = 8,         /* runtime_error "Config Error: ..." (src/IO/ConfigParser.cpp:36-294) */
+    QK_ERR_STATE = 9          /* call out of order (e.g. poll of an unknown ticket) */
+} qk_status;
+
+/* ---------------------------------------------------------------- enums
+ * Same order as quantkos::Implemented (include/core/config/ConfigFileEnums.hpp:24-124). */
+typedef enum qk_model { QK_HESTON = 0, QK_BATES = 1 } qk_model;
+typedef enum qk_scheme { QK_EULER = 0, QK_IMPLICIT_MILSTEIN = 1, QK_ANDERSEN_QE = 2 } qk_scheme;
+typedef enum qk_opt_type {
+    QK_EUROPEAN = 0,
+    QK_ASIAN = 1,
+    QK_BARRIER_UP_OUT = 2,
+    QK_BARRIER_DOWN_OUT = 3,
+    QK_BARRIER_UP_IN = 4,
+    QK_BARRIER_DOWN_IN = 5,
+    QK_LOOKBACK_FLOATING = 6,
+    QK_LOOKBACK_FIXED = 7,
+    QK_BINARY_CASH = 8,
+    QK_BINARY_ASSET = 9,
+    QK_AMERICAN = 10
+} qk_opt_type;
+typedef enum qk_right { QK_CALL = 0, QK_PUT = 1 } qk_right;
+typedef enum qk_precision { QK_FP64 = 0, QK_FP32 = 1 } qk_precision;
+/* Longstaff-Schwartz regression basis.
+ *  QK_LSM_LAGUERRE3: the reference's LaguerreP03 on X = S/K, 4 terms, every step an
+ *                    exercise date, Tikhonov 1e-8 + Cholesky + mean fallback
+ *                    (include/core/options/LSMAmerican.hpp:157-613);
+ *  QK_LSM_POLY_SV:   {1, S, S^2, S^3, v, S*v} on S/K-scaled values, ITM paths, FP64
+ *                    Cholesky of the centred and scaled Gram, pivoted QR when the
+ *                    condition estimate exceeds 1e8 (no reference counterpart). */
+typedef enum qk_lsm_basis { QK_LSM_LAGUERRE3 = 0, QK_LSM_POLY_SV = 1 } qk_lsm_basis;
+
+/* ---------------------------------------------------------------- contract
+ * One pricing request.  Mirrors quantkos::Config::UInputs (include/core/config/Config.hpp:677-775)
+ * restricted to what the hot path reads.  Monetary inputs are in real units; the
+ * engine applies UInputs::apply_price_scaling (Config.hpp:710-723) itself when
+ * `normalize` is set and scales results back (OptionPricer.hpp:323-332). */
+typedef struct qk_payoff {
+    int32_t type;   /* qk_opt_type */
+    int32_t right;  /* qk_right */
+    double strike;  /* K */
+    double barrier; /* B (barrier types only) */
+} qk_payoff;
+
+typedef struct qk_contract {
+    double S0, v0, r, q;                          /* MarketConfig */
+    int32_t model, scheme;                        /* qk_model, qk_scheme */
+    double kappa, theta, sigma, rho;              /* MathModelConfig::Heston */
+    double lambda_j, mu_j, sigma_j;               /* MathModelConfig::Bates (ignored for Heston) */
+    double psi_c;                                 /* QE switching level; 0 means 1.5 (MSchemes.hpp:290) */
+    double T;                                     /* TimeConfig::t_end */
+    int32_t n_steps;                              /* TimeConfig::N_time_steps (= ceil(T/dt)) */
+    int32_t normalize;                            /* MCConfig::normalize_prices */
+    int64_t n_paths;                              /* MCConfig::N_Paths */
+    uint64_t seed;                                /* MCConfig::rng_seed (Philox key) */
+    uint64_t stream;                              /* common-random-number stream id (Philox counter word) */
+    int32_t precision;                            /* qk_precision for the path stepping */
+    int32_t n_payoffs;                            /* 1..QK_MAX_PAYOFFS, all priced in one pass */
+    qk_payoff payoffs[QK_MAX_PAYOFFS];
+    int32_t lsm_basis;                            /* qk_lsm_basis (American only) */
+    int32_t lsm_dates;                            /* exercise dates; 0 = every time step (American only) */
+} qk_contract;
+
+/* Finite-difference Greeks by re-pricing under common random numbers
+ * (execute_mc_framework, include/core/engine/MCEngine.hpp:576-735). */
+#define QK_GREEK_DELTA_GAMMA 1
+#define QK_GREEK_VEGA_VOMMA 2
+#define QK_GREEK_VANNA 4
+#define QK_GREEK_RHO 8
+#define QK_GREEK_THETA 16
+#define QK_GREEK_ALL 31
+typedef struct qk_greeks {
+    int32_t mask;       /* QK_GREEK_* bits (MCConfig compute_* flags, Config.hpp:409-417) */
+    int32_t vega_mode;  /* 0: absolute bump of sqrt(v0) (reference, MCEngine.hpp:611-632);
+                           1: relative bump of v0, vega/vomma/vanna reported per unit of v0 */
+    double bump_S_rel;  /* spot_price_relative_bump_size, default 0.001 */
+    double bump_vol;    /* vega_mode 0: volatility_absolute_bump_size (0.01); mode 1: relative v0 bump */
+    double bump_r_abs;  /* risk_free_rate_absolute_bump_size, default 1e-4 */
+    double bump_T_abs;  /* time_absolute_bump_size, default 1/365 */
+} qk_greeks;
+
+typedef struct qk_payoff_result {
+    double price;     /* MCOpPrices::option_price (OptionPricer.hpp:50-70) */
+    double std_error; /* MCOpPrices::standard_error */
+    double prob_itm;  /* MCOpPrices::prob_itm */
+    double delta, gamma, vega, vomma, vanna, rho, theta; /* MCGreeks (MCEngine.hpp:93-120) */
+} qk_payoff_result;
+
+typedef struct qk_result {
+    int32_t status;     /* qk_status of this contract */
+    int32_t n_payoffs;
+    int64_t n_paths;
+    double path_steps;  /* path-steps simulated for this contract, bumps included */
+    qk_payoff_result p[QK_MAX_PAYOFFS];
+} qk_result;
+
+/* Device timings of the most recent pricing call on a handle (CUDA events on the handle's stream). */
+typedef struct qk_timing {
+    double device_ms;     /* first kernel start to last kernel end */
+    double paths_ms;      /* path-generation kernels */
+    double reduce_ms;     /* merge / LSM regression kernels */
+    int64_t launches;     /* kernels launched by the call */
+    double path_steps;    /* path-steps simulated */
+    int64_t h2d_bytes;    /* host-to-device bytes the call copied (descriptors) */
+    int64_t d2h_bytes;    /* device-to-host bytes the call copied (results) */
+} qk_timing;
+
+typedef struct qk_handle qk_handle;
+
+/* ---------------------------------------------------------------- lifecycle */
+const char *qk_version(void);
+/* Thread-local message of the last failing call on this thread. */
+const char *qk_last_error(void);
+/* Replaces Kokkos::initialize + the per-run Memory classes (app/main.cpp:78;
+ * PathsMCBatchMem.hpp:330-372): binds `device`, creates a stream and the
+ * handle-owned device arenas. */
+qk_status qk_create(int32_t device, qk_handle **out);
+qk_status qk_destroy(qk_handle *h);
+/* The CUDA stream (cudaStream_t) all work of the handle is queued on. */
+qk_status qk_get_stream(qk_handle *h, void **stream);
+qk_status qk_last_timing(const qk_handle *h, qk_timing *out);
+/* Measured SFU (MUFU) throughput of the device, in operations per second: a
+ * kernel of independent ex2.approx chains on every SM, timed with CUDA events.
+ * The roofline denominator of the fused path kernels, which are SFU/issue-bound. */
+qk_status qk_measure_sfu(qk_handle *h, double *mufu_ops_per_s);
+/* Host-side validation with the reference's rules (UInputs::validate, Config.hpp:694-704). */
+qk_status qk_validate(const qk_contract *c, const qk_greeks *g);
+
+/* ---------------------------------------------------------------- pricing
+ * qk_price_plain — the plain method, the drop-in: one contract, one all-FP64
+ * path kernel launch (plus its reduction), like one
+ * MCDispatcher(UInputs).launch_montecarlo() (include/core/engine/Distpatcher.hpp:78)
+ * with every Greek bump a further launch (MCEngine.hpp:586-730).  `c->precision`
+ * is ignored (FP64).  `g` may be NULL. */
+qk_status qk_price_plain(qk_handle *h, const qk_contract *c, const qk_greeks *g, qk_result *out);
+
+/* qk_price_batch — the batched mixed-precision engine: all contracts and all
+ * their Greek bumps go into one persistent kernel through a device queue of
+ * (task, path-block) tiles; FP32 stepping unless a contract asks for FP64;
+ * FP64 accumulation.  American contracts run the device-resident LSM.  Replaces a
+ * host loop of MCDispatcher runs; `out` has `n` entries. */
+qk_status qk_price_batch(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g, qk_result *out);
+
+/* Device-resident form of qk_price_batch for callers that reprice the same set:
+ * prepare uploads the task/tile descriptors once, run queues the kernels
+ * (asynchronously, on the handle's stream), fetch waits and fills `out`. */
+qk_status qk_batch_prepare(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g);
+qk_status qk_batch_run(qk_handle *h);
+qk_status qk_batch_fetch(qk_handle *h, qk_result *out, int32_t n);
+
+/* ---------------------------------------------------------------- parity harness
+ * qk_step_trace — SDEScheme<M,S>::evolve_step with fed draws
+ * (include/core/schemes/markovian/MSchemes.hpp:133-156, 229-253, 363-442, 493-526),
+ * run on the device by the same step code the pricing kernels use.
+ * Per step i: z[3i..3i+2] = {Z1, Z2, Zjump}; u[umax*i ..] = Poisson uniforms in the
+ * order Knuth's loop consumes them.  Starts from (c->S0, c->v0) as given, dt = c->T / n_steps.
+ * precision: qk_precision.  Returns QK_ERR_INVALID_ARG if a step needs more than umax uniforms. */
+qk_status qk_step_trace(int32_t precision, const qk_contract *c, const double *z, const double *u, int32_t umax,
+                        int32_t n_steps, double *S_out, double *v_out);
+
+/* qk_paths_dump — the spot paths of paths [first, first+count) of contract `c` as the
+ * pricing kernels generate them (same Philox counters), row-major count x n_steps
+ * (the .paths payload layout, include/IO/IOBinary.hpp:96-249), FP64 output. */
+qk_status qk_paths_dump(qk_handle *h, const qk_contract *c, int64_t first, int64_t count, double *S_out,
+                        double *v_out);
+
+/* ---------------------------------------------------------------- configuration
+ * qk_config mirrors quantkos::Config::UInputs (include/core/config/Config.hpp:677-775)
+ * field by field; qk_config_parse_file is Parser::parse (src/IO/ConfigParser.cpp:36-294)
+ * for the same YAML files (blocks Market, Options, Model{Heston|Bates}, Numerics,
+ * Time, MC, Output; unknown keys ignored, as there).  Keys this engine adds, all
+ * optional: MC.Precision (FP64 | FP32), MC.Engine (plain | batch),
+ * MC.LSM_Basis (Laguerre3 | PolySV), MC.LSM_Dates (int), MC.Vega_Mode (0 | 1),
+ * MC.Stream (int). */
+typedef struct qk_config {
+    double S0, v0, r, q;                                        /* MarketConfig */
+    int32_t opt_type, opt_right;                                /* OptionsConfig */
+    double K, B;
+    int32_t model;                                              /* MathModelConfig::id_model */
+    double heston_k, heston_theta, heston_sigma, heston_rho;    /* MathModelConfig::Heston */
+    double bates_k, bates_theta, bates_sigma, bates_rho;        /* MathModelConfig::Bates */
+    double bates_lambda, bates_mu, bates_sigma_j;
+    int32_t scheme;                                             /* NumSchemeConfig */
+    double t_end, inp_dt, dt;                                   /* TimeConfig */
+    int32_t n_steps;
+    int32_t normalize, n_paths, batch_size;                     /* MCConfig */
+    uint64_t seed;
+    int64_t max_vram_mb, max_cpu_ram_mb;
+    int32_t analyze_distribution;
+    int32_t greeks_mask;
+    double bump_S_rel, bump_vol_abs, bump_r_abs, bump_T_abs;
+    int32_t verbosity, format;                                  /* OutputConfig */
+    char out_dir[256], paths_file[256], log_file[256];
+    int32_t precision, engine, lsm_basis, lsm_dates, vega_mode; /* engine extensions */
+    uint64_t stream;
+} qk_config;
+
+/* Defaults of UInputs (Config.hpp:50-623) plus engine extensions (FP64, plain). */
+qk_status qk_config_default(qk_config *out);
+/* Parse + validate (Parser::parse ends with UInputs::validate). */
+qk_status qk_config_parse_file(const char *path, qk_config *out);
+qk_status qk_config_parse_string(const char *yaml, qk_config *out);
+/* UInputs::validate: checks and fills n_steps = ceil(t_end / inp_dt), dt = t_end / n_steps. */
+qk_status qk_config_validate(qk_config *c);
+/* The contract and Greeks request a validated config prices (MCDispatcher's dispatch). */
+qk_status qk_config_to_contract(const qk_config *c, qk_contract *out, qk_greeks *g);
+/* MCDispatcher(UInputs).launch_montecarlo() (include/core/engine/Distpatcher.hpp:78):
+ * prices the config with the plain (FP64) or batched engine per c->engine, writes
+ * the .paths file when c->paths_file is set, fills the payoff percentiles when
+ * analyze_distribution is set (pct[15]: p0 p1 p5 p10 p20 p30 p40 p50 p60 p70 p80
+ * p90 p95 p99 p100, discounted and scaled as OptionPricer.hpp:340-360). */
+qk_status qk_run_config(qk_handle *h, const qk_config *c, qk_result *out, double *pct);
+
+/* ---------------------------------------------------------------- serving
+ * A continuous-batching request loop.  Requests are admitted by the HBM their
+ * LSM slabs and partials need (budget in MiB; 0 = 80% of free HBM), batched with
+ * whatever else has arrived, and their results polled by ticket. */
+typedef struct qk_server qk_server;
+typedef struct qk_serve_stats {
+    int64_t submitted, completed, rejected;
+    double p50_ms, p99_ms, p999_ms, max_ms;
+    double contracts_per_s, path_steps_per_s;
+    int64_t batches;
+    double busy_s;
+} qk_serve_stats;
+qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch, qk_server **out);
+qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g, int64_t *ticket);
+/* done = 1 and *out filled once the ticket finished; wait_ms bounds the wait (0 = poll). */
+qk_status qk_serve_poll(qk_server *s, int64_t ticket, int32_t wait_ms, int32_t *done, qk_result *out);
+qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out);
+qk_status qk_serve_stop(qk_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUANTKOS_B200_H */

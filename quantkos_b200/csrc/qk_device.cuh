@@ -1,0 +1,365 @@
+// Device building blocks of the Monte Carlo hot path (sm_100a).
+//
+//   * Philox4x32-10 counter-based generator and the fixed draw layout that makes
+//     every path reproducible whatever the launch shape;
+//   * the Heston / Bates step functions under Euler, implicit Milstein and
+//     Andersen QE, written once, templated on the arithmetic type and on the
+//     draw source (Philox in the pricing kernels, fed draws in the parity trace);
+//   * payoff trackers and final payoffs for the ten forward option types;
+//   * FP64 statistics helpers (Welford / Chan merge).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "qk_internal.h"
+
+namespace qk {
+
+// ============================================================================
+// Philox4x32-10 (J. Salmon, M. Moraes, R. Dror, D. Shaw, "Parallel random
+// numbers: as easy as 1, 2, 3", SC'11): 10 rounds of two 32x32->64 multiplies
+// with a Weyl-sequence key schedule.  Counter = (block, path, stream, domain),
+// key = (lo32(seed), hi32(seed)).
+// ============================================================================
+struct U4 {
+    uint32_t x, y, z, w;
+};
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = kPhiloxM0 * c.x;
+        const uint32_t hi0 = __umulhi(kPhiloxM0, c.x);
+        const uint32_t lo1 = kPhiloxM1 * c.z;
+        const uint32_t hi1 = __umulhi(kPhiloxM1, c.z);
+        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+        k0 += kPhiloxW0;
+        k1 += kPhiloxW1;
+    }
+    return c;
+}
+
+// ============================================================================
+// Arithmetic policy.  FP32 uses the SFU (MUFU) approximations explicitly;
+// FP64 uses the correctly-rounded / IEEE CUDA library functions.
+// ============================================================================
+template <class R>
+struct Math;
+
+template <>
+struct Math<float> {
+    static __device__ __forceinline__ float exp(float x) { return __expf(x); }
+    static __device__ __forceinline__ float log(float x) { return __logf(x); }
+    // sqrt through one MUFU.RSQ; arguments here are >= 0 (variances, moment ratios)
+    static __device__ __forceinline__ float sqrt(float x) { return x > 1.0e-36f ? x * rsqrtf(x) : 0.0f; }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float erf(float x) { return erff(x); }
+    // uniform in (0,1): (k + 1/2) / 2^23, k = top 23 bits of the word
+    static __device__ __forceinline__ float u01(uint32_t w) {
+        return __fmaf_rn(static_cast<float>(w >> 9), 1.0f / 8388608.0f, 1.0f / 16777216.0f);
+    }
+    // Box-Muller pair: R = sqrt(-2 ln u1), angle = 2*pi*(u2 - 1/2)
+    static __device__ __forceinline__ void box_muller(uint32_t w1, uint32_t w2, float &z1, float &z2) {
+        const float u1 = u01(w1);
+        const float u2 = u01(w2);
+        const float rad = sqrt(-2.0f * log(u1));
+        float s, c;
+        __sincosf(6.28318530717958648f * (u2 - 0.5f), &s, &c);
+        z1 = rad * c;
+        z2 = rad * s;
+    }
+};
+
+template <>
+struct Math<double> {
+    static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+    static __device__ __forceinline__ double log(double x) { return ::log(x); }
+    static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double erf(double x) { return ::erf(x); }
+    static __device__ __forceinline__ double u01(uint32_t w) {
+        return (static_cast<double>(w) + 0.5) * (1.0 / 4294967296.0);
+    }
+    static __device__ __forceinline__ void box_muller(uint32_t w1, uint32_t w2, double &z1, double &z2) {
+        const double u1 = u01(w1);
+        const double u2 = u01(w2);
+        const double rad = ::sqrt(-2.0 * ::log(u1));
+        double s, c;
+        ::sincospi(2.0 * u2 - 1.0, &s, &c);
+        z1 = rad * c;
+        z2 = rad * s;
+    }
+};
+
+template <class R>
+__device__ __forceinline__ R rmax(R a, R b) { return fmax(a, b); }
+template <class R>
+__device__ __forceinline__ R rmin(R a, R b) { return fmin(a, b); }
+
+// ============================================================================
+// Draw sources.  A step asks for: one normal pair (Z1, Z2); Bates steps then ask
+// for Poisson uniforms one at a time and, when a jump occurred, one jump normal.
+//
+// Philox layout per path p of stream s:
+//   Heston: block floor(n/2), domain 0; words (x,y) feed step 2k, (z,w) step 2k+1.
+//   Bates:  block n, domain 0: (x,y) -> normal pair, z -> 1st Poisson uniform,
+//           w -> 2nd Poisson uniform; block n, domain 1: (x,y) -> jump normal,
+//           (z,w) -> Poisson uniforms 3,4; block n, domain d>=2: uniforms 4d-3 .. 4d.
+// ============================================================================
+template <class R>
+struct PhiloxBatesStep {
+    uint32_t k0, k1, path, stream;
+    int step;
+    U4 w0;      // domain-0 words of this step
+    U4 wx;      // current extra-domain block
+    int used;   // Poisson uniforms consumed in this step
+    int domain; // extra domain currently held in wx (0 = none)
+
+    __device__ __forceinline__ void normal_pair(R &z1, R &z2) { Math<R>::box_muller(w0.x, w0.y, z1, z2); }
+    __device__ __forceinline__ U4 extra(int d) {
+        return philox4x32_10(U4{static_cast<uint32_t>(step), path, stream, static_cast<uint32_t>(d)}, k0, k1);
+    }
+    __device__ __forceinline__ R uniform() {
+        const int k = used++;
+        if (k == 0) return Math<R>::u01(w0.z);
+        if (k == 1) return Math<R>::u01(w0.w);
+        // uniform k (0-based) >= 2: domain 1 words z,w for k = 2,3; domain 2 + (k-4)/4 words x..w after
+        const int d = (k < 4) ? 1 : 2 + (k - 4) / 4;
+        if (domain != d) {
+            wx = extra(d);
+            domain = d;
+        }
+        const int slot = (k < 4) ? k : ((k - 4) & 3);
+        const uint32_t word = slot == 0 ? wx.x : (slot == 1 ? wx.y : (slot == 2 ? wx.z : wx.w));
+        return Math<R>::u01(word);
+    }
+    __device__ __forceinline__ R jump_normal() {
+        const U4 j = extra(1);
+        R z1, z2;
+        Math<R>::box_muller(j.x, j.y, z1, z2);
+        return z1;
+    }
+};
+
+// Fed draws for the parity trace: z[3] = {Z1, Z2, Zjump}; u[umax] Poisson uniforms.
+template <class R>
+struct FedStep {
+    const double *z;
+    const double *u;
+    int umax;
+    int used;
+    int overflow;
+    __device__ __forceinline__ void normal_pair(R &z1, R &z2) {
+        z1 = static_cast<R>(z[0]);
+        z2 = static_cast<R>(z[1]);
+    }
+    __device__ __forceinline__ R uniform() {
+        if (used >= umax) {
+            overflow = 1;
+            return R(0);
+        }
+        return static_cast<R>(u[used++]);
+    }
+    __device__ __forceinline__ R jump_normal() { return static_cast<R>(z[2]); }
+};
+
+// ============================================================================
+// Scheme steps.  Each follows the reference's evolve_step line for line; the
+// only rewrite is QE's quadratic-branch martingale term, where
+// log(exp(X)/sqrt(t)) is evaluated as X - log(t)/2 (the same quantity without
+// an exp/rsqrt/log round trip).
+// ============================================================================
+
+// Heston + Euler: include/core/schemes/markovian/MSchemes.hpp:133-156
+template <class R>
+__device__ __forceinline__ void step_euler(const StepConst<R> &p, R &S, R &v, R Z1, R Z2) {
+    const R Zv = Z1;
+    const R ZS = p.rho * Z1 + p.rho_c * Z2;
+    const R sqv = Math<R>::sqrt(v);
+    const R ex = p.r_minus_q_dt - v * p.half_dt + (sqv * p.sqrt_dt) * ZS;
+    const R Sn = S * Math<R>::exp(ex);
+    const R vn = v * p.one_minus_k_dt + p.k_theta_dt + (p.sigma_sqrt_dt * sqv) * Zv;
+    S = Sn;
+    v = rmax(vn, R(0));
+}
+
+// Heston + implicit Milstein: MSchemes.hpp:229-253
+template <class R>
+__device__ __forceinline__ void step_milstein(const StepConst<R> &p, R &S, R &v, R Z1, R Z2) {
+    const R Zv = Z1;
+    const R ZS = p.rho * Z1 + p.rho_c * Z2;
+    const R sqv = Math<R>::sqrt(v);
+    const R ex = p.r_minus_q_dt - v * p.half_dt + (sqv * p.sqrt_dt) * ZS;
+    const R Sn = S * Math<R>::exp(ex);
+    const R corr = p.quarter_sigma_sq_dt * (Zv * Zv - R(1));
+    const R vn = p.implicit_den * (v + p.k_theta_dt + (p.sigma_sqrt_dt * sqv) * Zv + corr);
+    S = Sn;
+    v = rmax(vn, R(0));
+}
+
+// Heston + Andersen QE with martingale correction: MSchemes.hpp:363-442
+template <class R>
+__device__ __forceinline__ void step_qe(const StepConst<R> &p, R &S, R &v, R Zv, R Zind) {
+    const R m = v * p.exp_mkdt + p.theta_m;
+    const R s2 = v * p.s2f1 + p.s2f2;
+    R vn;
+    R logM;  // log of the martingale factor M
+    if (m <= p.eps) {
+        vn = R(0);
+        logM = R(0);
+    } else {
+        const R inv_m = Math<R>::div(R(1), m);
+        const R psi = s2 * inv_m * inv_m;
+        if (psi <= p.eps) {
+            vn = m;
+            logM = R(0);
+        } else if (psi <= p.psi_c) {
+            const R two_ip = Math<R>::div(R(2), psi);
+            const R b2 = two_ip - R(1) + Math<R>::sqrt(two_ip * (two_ip - R(1)));
+            const R a = Math<R>::div(m, R(1) + b2);
+            const R bz = Math<R>::sqrt(b2) + Zv;
+            vn = a * bz * bz;
+            // 0.5/a = 0.5 (1 + b2) / m
+            const R safe_A = rmin(p.A, R(0.5) * (R(1) + b2) * inv_m - p.eps);
+            const R term = R(1) - R(2) * safe_A * a;
+            // M = exp(A b2 a / term) / sqrt(term)  =>  log M = A b2 a / term - log(term) / 2
+            logM = Math<R>::div(safe_A * b2 * a, term) - R(0.5) * Math<R>::log(term);
+        } else {
+            const R pz = Math<R>::div(psi - R(1), psi + R(1));
+            const R beta = (R(1) - pz) * inv_m;
+            const R U = R(0.5) * (R(1) + Math<R>::erf(Zv * p.inv_sqrt2));
+            if (U <= pz) {
+                vn = R(0);
+            } else {
+                const R safe_U = rmin(U, R(1) - p.eps);
+                vn = Math<R>::div(Math<R>::log(Math<R>::div(R(1) - pz, R(1) - safe_U)), beta);
+            }
+            const R safe_A = rmin(p.A, beta - p.eps);
+            const R M = pz + Math<R>::div(beta * (R(1) - pz), beta - safe_A);
+            logM = Math<R>::log(M);
+        }
+    }
+    const R K0 = -logM - p.K1_half_K3 * v;
+    const R isig = p.K3 * v + p.K4 * vn;
+    const R ex = p.r_minus_q_dt + K0 + (p.K1 * v + p.K2 * vn) + Math<R>::sqrt(isig) * Zind;
+    S = S * Math<R>::exp(ex);
+    v = vn;
+}
+
+template <class R, int SCHEME>
+__device__ __forceinline__ void heston_step(const StepConst<R> &p, R &S, R &v, R Z1, R Z2) {
+    if constexpr (SCHEME == kEuler) {
+        step_euler<R>(p, S, v, Z1, Z2);
+    } else if constexpr (SCHEME == kMilstein) {
+        step_milstein<R>(p, S, v, Z1, Z2);
+    } else {
+        step_qe<R>(p, S, v, Z1, Z2);
+    }
+}
+
+// Bates jump part after the (drift-compensated) Heston step: MSchemes.hpp:493-526.
+// Knuth's Poisson draw: multiply uniforms until the product drops below exp(-lambda dt).
+template <class R, class Draws>
+__device__ __forceinline__ void bates_jump(const StepConst<R> &p, R &S, Draws &d) {
+    R prod = d.uniform();
+    if (prod >= p.exp_m_lambda_dt) {
+        int N = 0;
+        do {
+            ++N;
+            prod *= d.uniform();
+        } while (prod >= p.exp_m_lambda_dt && N < kMaxJumpsPerStep);
+        const R Z = d.jump_normal();
+        const R rN = static_cast<R>(N);
+        const R mag = Math<R>::exp(rN * p.mu_j + Math<R>::sqrt(rN) * p.sigma_j * Z);
+        S *= mag;
+    }
+}
+
+template <class R, int MODEL, int SCHEME, class Draws>
+__device__ __forceinline__ void evolve_step(const StepConst<R> &p, R &S, R &v, Draws &d) {
+    R Z1, Z2;
+    d.normal_pair(Z1, Z2);
+    heston_step<R, SCHEME>(p, S, v, Z1, Z2);
+    if constexpr (MODEL == kBates) bates_jump<R>(p, S, d);
+}
+
+// ============================================================================
+// Payoffs: include/core/options/Payoff.hpp:35-243.  Trackers (running sum in
+// double, running max / min started at S0) are kept for every path; the final
+// payoff per requested contract leg reads the ones it needs.
+// ============================================================================
+template <class R>
+__device__ __forceinline__ R intrinsic(int right, R S, R K) {
+    return right == kCall ? (S > K ? S - K : R(0)) : (K > S ? K - S : R(0));
+}
+
+template <class R>
+__device__ __forceinline__ R final_payoff(const PayoffSpec &ps, R S, double ssum, R smax, R smin, int n_steps) {
+    const R K = static_cast<R>(ps.K);
+    const R B = static_cast<R>(ps.B);
+    switch (ps.type) {
+        case kEuropean: return intrinsic<R>(ps.right, S, K);
+        case kAsian: return intrinsic<R>(ps.right, static_cast<R>(ssum / static_cast<double>(n_steps)), K);
+        case kBarrierUpOut: return smax < B ? intrinsic<R>(ps.right, S, K) : R(0);
+        case kBarrierDownOut: return smin > B ? intrinsic<R>(ps.right, S, K) : R(0);
+        case kBarrierUpIn: return smax >= B ? intrinsic<R>(ps.right, S, K) : R(0);
+        case kBarrierDownIn: return smin <= B ? intrinsic<R>(ps.right, S, K) : R(0);
+        case kLookbackFloating:
+            return ps.right == kCall ? intrinsic<R>(kCall, S, smin) : intrinsic<R>(kPut, S, smax);
+        case kLookbackFixed:
+            return ps.right == kCall ? intrinsic<R>(kCall, smax, K) : intrinsic<R>(kPut, smin, K);
+        case kBinaryCash:
+            return ps.right == kCall ? (S > K ? R(1) : R(0)) : (S < K ? R(1) : R(0));
+        case kBinaryAsset:
+            return ps.right == kCall ? (S > K ? S : R(0)) : (S < K ? S : R(0));
+        default: return intrinsic<R>(ps.right, S, K);  // American legs priced at maturity only here
+    }
+}
+
+// ============================================================================
+// FP64 statistics: (n, mean, M2) merged with Chan et al.'s parallel update.
+// ============================================================================
+__device__ __forceinline__ Moments chan_merge(const Moments &a, const Moments &b) {
+    const double n = a.n + b.n;
+    if (n <= 0.0) return Moments{0.0, 0.0, 0.0, 0.0};
+    if (a.n <= 0.0) return b;
+    if (b.n <= 0.0) return a;
+    const double d = b.mean - a.mean;
+    Moments r;
+    r.n = n;
+    r.mean = a.mean + d * (b.n / n);
+    r.m2 = a.m2 + b.m2 + d * d * (a.n * b.n / n);
+    r.itm = a.itm + b.itm;
+    return r;
+}
+
+__device__ __forceinline__ Moments shfl_down_moments(const Moments &m, int off) {
+    Moments r;
+    r.n = __shfl_down_sync(0xffffffffu, m.n, off);
+    r.mean = __shfl_down_sync(0xffffffffu, m.mean, off);
+    r.m2 = __shfl_down_sync(0xffffffffu, m.m2, off);
+    r.itm = __shfl_down_sync(0xffffffffu, m.itm, off);
+    return r;
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    return x;
+}
+
+// Exact two-pass moments of the 32 values of a warp (inactive lanes excluded):
+// the values are in registers, so the second pass costs one more shuffle tree.
+__device__ __forceinline__ Moments warp_moments(double x, bool active, bool itm) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    const unsigned im = __ballot_sync(0xffffffffu, active && itm);
+    const double n = static_cast<double>(__popc(act));
+    const double s = warp_sum(active ? x : 0.0);
+    const double mean = n > 0.0 ? s / n : 0.0;
+    const double dv = active ? x - mean : 0.0;
+    const double m2 = warp_sum(dv * dv);
+    return Moments{n, mean, m2, static_cast<double>(__popc(im))};
+}
+
+}  // namespace qk

@@ -1,0 +1,101 @@
+// Host engine state: the opaque qk_handle, device/pinned arenas, and the plan
+// (task list) of one pricing call.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "qk_internal.h"
+
+namespace qk {
+
+// Grow-only device allocation owned by a handle (replaces the per-run Kokkos
+// Views of PathsMCBatchMem / BackwardLSMMemory: allocated once, reused).
+struct DevArena {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    qk_status ensure(size_t bytes);
+    void release();
+};
+
+// Grow-only pinned host staging buffer.
+struct HostArena {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    qk_status ensure(size_t bytes);
+    void release();
+};
+
+struct LsmTaskInfo {
+    int contract, role, grid;
+    int64_t n_paths;
+    double intrinsic0, eps;
+};
+
+struct Plan {
+    int n_contracts = 0;
+    bool plain = false;
+    std::vector<qk_greeks> greeks;     // per contract; mask 0 = no Greeks
+    const qk_greeks *g_of(int i) const { return greeks[i].mask ? &greeks[i] : nullptr; }
+    std::vector<qk_contract> norm;     // normalised contracts
+    std::vector<double> scale;         // price scale factor per contract
+    std::vector<int32_t> status;       // per-contract status
+    std::vector<TaskDev> tasks;        // forward tasks in schedule order
+    std::vector<int> task_contract, task_role;
+    std::vector<int> task_of;          // [contract * kNumRoles + role] -> task index or -1
+    std::vector<int> american;         // contracts priced by LSM
+    int64_t total_slots = 0;
+    int64_t total_records = 0;
+    double path_steps = 0.0;
+    double lsm_path_steps = 0.0;
+    std::vector<LsmTaskInfo> lsm_tasks;
+};
+
+// LSM working set of one task on the device.
+struct LsmArena {
+    DevArena slab_S, slab_v, cashflow, block_sums, coeffs, task, status;
+};
+
+}  // namespace qk
+
+struct qk_handle {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_paths0 = nullptr, ev_paths1 = nullptr, ev_end = nullptr;
+    qk::DevArena d_tasks, d_prefix, d_partials, d_moments, d_cursor, d_trace;
+    qk::HostArena h_tasks, h_moments, h_lsm;
+    qk::DevArena d_lsm_moments;
+    qk::LsmArena lsm;
+    qk::Plan plan;
+    bool prepared = false;
+    qk_timing timing{};
+    int64_t launches = 0;
+    int64_t h2d_bytes = 0, d2h_bytes = 0;
+    double lsm_ms = 0.0, lsm_paths_ms = 0.0;
+    int64_t lsm_launches = 0;
+};
+
+namespace qk {
+
+enum : int { kNumRoles = 12 };
+
+TaskDev make_task(const qk_contract &b, int ppt);
+qk_contract normalised(const qk_contract &c, double *scale);
+qk_contract bumped(const qk_contract &n, const qk_greeks *g, int role);
+std::vector<int> roles_for(const qk_greeks *g, double T);
+
+// Plan, run and assemble a set of contracts; `gs` holds one Greeks request per
+// contract (or NULL).  Used by qk_price_* and by the serving lanes.
+qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *gs, qk_result *out, bool plain);
+
+// Every path's leg-0 payoff (undiscounted, normalised) of a contract, on the host.
+qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &out);
+
+// Longstaff-Schwartz for the American contracts of a plan (qk_lsm.cu).
+qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Moments> &moments);
+void assemble_lsm_results(qk_handle *h, const Plan &plan, const std::vector<Moments> &moments, qk_result *out);
+void lsm_release(qk_handle *h);
+
+}  // namespace qk

@@ -1,0 +1,710 @@
+// Longstaff-Schwartz American pricing, fully device-resident (sm_100a).
+//
+// Reference path (paths relative to the reference project): the forward pass
+// stores every path to a host master matrix (include/core/memory/LSMMemory.hpp:145-183),
+// then a host loop streams one time slice per step over PCIe, reduces the
+// regression sums on the device, solves a Cholesky on the host and updates the
+// cash flows (include/core/engine/ForwardBackwardMC.hpp:204-255,
+// include/core/options/LSMAmerican.hpp:252-613).
+//
+// Here: the forward kernel writes spot (and variance) only at the exercise
+// dates, as SoA slabs slab[date][path] in HBM; the backward sweep is one kernel
+// per date that applies the exercise decision of date d and accumulates the
+// regression sums of date d-1 in the same pass; a one-block kernel reduces the
+// block sums and solves the normal equations in FP64 on the device.  No host
+// round trip happens inside the sweep.
+//
+// Two regression modes:
+//   QK_LSM_LAGUERRE3 — the reference's: X = S/K, Laguerre L0..L3 (LSMAmerican.hpp:157-199),
+//     ITM paths, Tikhonov 1e-8 on the diagonal, Cholesky with a 1e-14 pivot floor and
+//     the mean fallback (LSMAmerican.hpp:516-613);
+//   QK_LSM_POLY_SV — basis {1, S, S^2, S^3, v, S v} on S/K-scaled values, evaluated in the
+//     shifted coordinates x = S/K - c_x(d), w = v - c_v(d) (same span), FP64 Cholesky of
+//     the Jacobi-scaled Gram, Householder QR with column pivoting when the Cholesky
+//     condition estimate exceeds 1e8, mean fallback below 6 ITM paths.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "qk_device.cuh"
+#include "qk_engine.h"
+#include "qk_host.h"
+#include "qk_kernels.h"
+
+namespace qk {
+
+constexpr int kLsmBlock = 256;
+constexpr int kMaxCoef = 8;
+
+template <int BASIS>
+struct BasisTraits;
+template <>
+struct BasisTraits<QK_LSM_LAGUERRE3> {
+    static constexpr int NB = 4;
+};
+template <>
+struct BasisTraits<QK_LSM_POLY_SV> {
+    static constexpr int NB = 6;
+};
+template <int NB>
+struct Sums {
+    static constexpr int NSUM = NB * (NB + 1) / 2 + NB + 1;  // upper Gram, rhs, count
+};
+
+struct LsmArgs {
+    int64_t N, ld;
+    int right;
+    int n_dates;
+    double K;     // normalised strike
+    double disc;  // exp(-r * date spacing)
+};
+
+template <class R>
+__device__ __forceinline__ R lsm_intrinsic(int right, R S, R K) {
+    return right == kCall ? (S > K ? S - K : R(0)) : (K > S ? K - S : R(0));
+}
+
+// Basis values of one path at one date.
+template <class R, int BASIS>
+__device__ __forceinline__ void eval_basis(R S, R v, R K, double cx, double cv, R *b) {
+    if constexpr (BASIS == QK_LSM_LAGUERRE3) {
+        // LaguerreBasis<4>::evaluate, Horner form (LSMAmerican.hpp:183-192)
+        const R X = S / K;
+        b[0] = R(1);
+        b[1] = R(1) - X;
+        b[2] = ((R(0.5) * X - R(2)) * X) + R(1);
+        b[3] = (((static_cast<R>(-1.0 / 6.0) * X + R(1.5)) * X - R(3)) * X) + R(1);
+    } else {
+        const R x = S / K - static_cast<R>(cx);
+        const R w = v - static_cast<R>(cv);
+        b[0] = R(1);
+        b[1] = x;
+        b[2] = x * x;
+        b[3] = x * x * x;
+        b[4] = w;
+        b[5] = x * w;
+    }
+}
+
+// Expected value of holding: sum of coefficients times basis, in double (LSMAmerican.hpp:484-502).
+template <class R, int BASIS>
+__device__ __forceinline__ double continuation(const double *c, R S, R v, R K, double cx, double cv) {
+    constexpr int NB = BasisTraits<BASIS>::NB;
+    R b[NB];
+    eval_basis<R, BASIS>(S, v, K, cx, cv, b);
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) s += c[i] * static_cast<double>(b[i]);
+    return s;
+}
+
+// Backward sweep over one date pair.  init: cash flows start as the payoff at
+// date d_upd (maturity); otherwise the exercise decision of date d_upd is
+// applied with its solved coefficients.  Then, if d_gram >= 0, the ITM
+// regression sums of date d_gram are accumulated with Y = cf * disc.
+template <class R, int BASIS>
+__global__ void __launch_bounds__(kLsmBlock) lsm_sweep_kernel(LsmArgs a, const R *__restrict__ slab_S,
+                                                             const R *__restrict__ slab_v, R *__restrict__ cf,
+                                                             int d_upd, int init, int d_gram,
+                                                             const double *__restrict__ coeffs,
+                                                             const double *__restrict__ centre,
+                                                             double *__restrict__ block_sums) {
+    constexpr int NB = BasisTraits<BASIS>::NB;
+    constexpr int NSUM = Sums<NB>::NSUM;
+    const R K = static_cast<R>(a.K);
+    const R disc = static_cast<R>(a.disc);
+    double acc[NSUM];
+#pragma unroll
+    for (int j = 0; j < NSUM; ++j) acc[j] = 0.0;
+    double cu[NB];
+    double cxu = 0.0, cvu = 0.0, cxg = 0.0, cvg = 0.0;
+    if (!init) {
+#pragma unroll
+        for (int i = 0; i < NB; ++i) cu[i] = coeffs[d_upd * kMaxCoef + i];
+        cxu = centre[2 * d_upd];
+        cvu = centre[2 * d_upd + 1];
+    }
+    if (d_gram >= 0) {
+        cxg = centre[2 * d_gram];
+        cvg = centre[2 * d_gram + 1];
+    }
+    const bool use_v = BASIS == QK_LSM_POLY_SV;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < a.N; i += stride) {
+        R c;
+        const R S = slab_S[static_cast<int64_t>(d_upd) * a.ld + i];
+        const R iv = lsm_intrinsic<R>(a.right, S, K);
+        if (init) {
+            c = iv;
+        } else {
+            c = cf[i];
+            const R disc_c = c * disc;
+            if (iv > R(0)) {
+                const R v = use_v ? slab_v[static_cast<int64_t>(d_upd) * a.ld + i] : R(0);
+                const double hold = continuation<R, BASIS>(cu, S, v, K, cxu, cvu);
+                c = (static_cast<double>(iv) > hold) ? iv : disc_c;
+            } else {
+                c = disc_c;
+            }
+        }
+        cf[i] = c;
+        if (d_gram >= 0) {
+            const R Sg = slab_S[static_cast<int64_t>(d_gram) * a.ld + i];
+            const R ivg = lsm_intrinsic<R>(a.right, Sg, K);
+            if (ivg > R(0)) {
+                const R vg = use_v ? slab_v[static_cast<int64_t>(d_gram) * a.ld + i] : R(0);
+                const R Y = c * disc;
+                R b[NB];
+                eval_basis<R, BASIS>(Sg, vg, K, cxg, cvg, b);
+                int j = 0;
+#pragma unroll
+                for (int r = 0; r < NB; ++r) {
+                    const double br = static_cast<double>(b[r]);
+#pragma unroll
+                    for (int q = r; q < NB; ++q) acc[j++] += br * static_cast<double>(b[q]);
+                }
+#pragma unroll
+                for (int r = 0; r < NB; ++r) acc[j++] += static_cast<double>(b[r]) * static_cast<double>(Y);
+                acc[j] += 1.0;
+            }
+        }
+    }
+    if (d_gram < 0) return;
+    // block reduction of the NSUM sums
+    __shared__ double s_red[kLsmBlock / 32][NSUM];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NSUM; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) s_red[warp][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NSUM) {
+        double t = 0.0;
+        for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red[w][threadIdx.x];
+        block_sums[static_cast<int64_t>(blockIdx.x) * NSUM + threadIdx.x] = t;
+    }
+}
+
+// ---------------------------------------------------------------- FP64 solves
+// Reference solve: Tikhonov 1e-8, Cholesky, 1e-14 pivot floor, mean fallback
+// (LSMAmerican.hpp:516-613).  Returns 0 on success, 2 on fallback.
+template <int NB>
+__device__ int solve_reference(const double *sums, double *c) {
+    double M[NB][NB], B[NB], L[NB][NB];
+    int j = 0;
+    for (int r = 0; r < NB; ++r)
+        for (int q = r; q < NB; ++q) {
+            M[r][q] = sums[j];
+            M[q][r] = sums[j];
+            ++j;
+        }
+    for (int r = 0; r < NB; ++r) B[r] = sums[j++];
+    const double count = sums[j];
+    for (int i = 0; i < NB; ++i) c[i] = 0.0;
+    auto fallback = [&]() {
+        if (count > 0.0) c[0] = B[0] / count;
+        return 2;
+    };
+    if (count < static_cast<double>(NB)) return fallback();
+    for (int i = 0; i < NB; ++i) M[i][i] += 1e-8;
+    for (int i = 0; i < NB; ++i)
+        for (int k = 0; k < NB; ++k) L[i][k] = 0.0;
+    for (int i = 0; i < NB; ++i) {
+        for (int jj = 0; jj <= i; ++jj) {
+            double s = 0.0;
+            for (int k = 0; k < jj; ++k) s += L[i][k] * L[jj][k];
+            if (i == jj) {
+                const double val = M[i][i] - s;
+                if (val < 1e-14) return fallback();
+                L[i][i] = sqrt(val);
+            } else {
+                L[i][jj] = (M[i][jj] - s) / L[jj][jj];
+            }
+        }
+    }
+    double y[NB];
+    for (int i = 0; i < NB; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < i; ++k) s += L[i][k] * y[k];
+        y[i] = (B[i] - s) / L[i][i];
+    }
+    for (int i = NB - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int k = i + 1; k < NB; ++k) s += L[k][i] * c[k];
+        c[i] = (y[i] - s) / L[i][i];
+    }
+    return 0;
+}
+
+// Centred/scaled Gram: Jacobi scaling, Cholesky with a condition estimate
+// (max/min pivot)^2, Householder QR with column pivoting when that exceeds 1e8
+// or the Cholesky breaks down.  Returns 0 Cholesky, 1 QR, 2 mean fallback.
+template <int NB>
+__device__ int solve_scaled(const double *sums, double *c) {
+    double G[NB][NB], b[NB], D[NB];
+    int j = 0;
+    for (int r = 0; r < NB; ++r)
+        for (int q = r; q < NB; ++q) {
+            G[r][q] = sums[j];
+            G[q][r] = sums[j];
+            ++j;
+        }
+    for (int r = 0; r < NB; ++r) b[r] = sums[j++];
+    const double count = sums[j];
+    for (int i = 0; i < NB; ++i) c[i] = 0.0;
+    if (count < static_cast<double>(NB)) {
+        if (count > 0.0) c[0] = b[0] / count;
+        return 2;
+    }
+    for (int i = 0; i < NB; ++i) D[i] = G[i][i] > 0.0 ? sqrt(G[i][i]) : 1.0;
+    for (int r = 0; r < NB; ++r) {
+        b[r] /= D[r];
+        for (int q = 0; q < NB; ++q) G[r][q] /= (D[r] * D[q]);
+    }
+    // Cholesky
+    double L[NB][NB];
+    bool ok = true;
+    double lmin = 1e300, lmax = 0.0;
+    for (int i = 0; i < NB && ok; ++i) {
+        for (int jj = 0; jj <= i; ++jj) {
+            double s = G[i][jj];
+            for (int k = 0; k < jj; ++k) s -= L[i][k] * L[jj][k];
+            if (i == jj) {
+                if (!(s > 0.0)) {
+                    ok = false;
+                    break;
+                }
+                L[i][i] = sqrt(s);
+                lmin = fmin(lmin, L[i][i]);
+                lmax = fmax(lmax, L[i][i]);
+            } else {
+                L[i][jj] = s / L[jj][jj];
+            }
+        }
+    }
+    if (ok && (lmax / lmin) * (lmax / lmin) <= 1e8) {
+        double y[NB];
+        for (int i = 0; i < NB; ++i) {
+            double s = b[i];
+            for (int k = 0; k < i; ++k) s -= L[i][k] * y[k];
+            y[i] = s / L[i][i];
+        }
+        for (int i = NB - 1; i >= 0; --i) {
+            double s = y[i];
+            for (int k = i + 1; k < NB; ++k) s -= L[k][i] * c[k];
+            c[i] = s / L[i][i];
+        }
+        for (int i = 0; i < NB; ++i) c[i] /= D[i];
+        return 0;
+    }
+    // Householder QR with column pivoting on the scaled Gram (rank-revealing), then
+    // the basic solution of the truncated triangular system.
+    double A[NB][NB], rhs[NB], norms[NB];
+    int perm[NB];
+    for (int r = 0; r < NB; ++r) {
+        rhs[r] = b[r];
+        for (int q = 0; q < NB; ++q) A[r][q] = G[r][q];
+    }
+    for (int q = 0; q < NB; ++q) {
+        perm[q] = q;
+        double s = 0.0;
+        for (int r = 0; r < NB; ++r) s += A[r][q] * A[r][q];
+        norms[q] = s;
+    }
+    int rank = 0;
+    double r00 = 0.0;
+    for (int k = 0; k < NB; ++k) {
+        int best = k;
+        for (int q = k + 1; q < NB; ++q)
+            if (norms[q] > norms[best]) best = q;
+        if (best != k) {
+            for (int r = 0; r < NB; ++r) {
+                const double t = A[r][k];
+                A[r][k] = A[r][best];
+                A[r][best] = t;
+            }
+            const double tn = norms[k];
+            norms[k] = norms[best];
+            norms[best] = tn;
+            const int tp = perm[k];
+            perm[k] = perm[best];
+            perm[best] = tp;
+        }
+        double alpha = 0.0;
+        for (int r = k; r < NB; ++r) alpha += A[r][k] * A[r][k];
+        alpha = sqrt(alpha);
+        if (k == 0) r00 = alpha;
+        if (alpha <= 1e-10 * r00 || alpha == 0.0) break;
+        if (A[k][k] > 0.0) alpha = -alpha;
+        double vk[NB];
+        for (int r = 0; r < NB; ++r) vk[r] = (r >= k) ? A[r][k] : 0.0;
+        vk[k] -= alpha;
+        double vnorm2 = 0.0;
+        for (int r = k; r < NB; ++r) vnorm2 += vk[r] * vk[r];
+        if (vnorm2 > 0.0) {
+            for (int q = k; q < NB; ++q) {
+                double s = 0.0;
+                for (int r = k; r < NB; ++r) s += vk[r] * A[r][q];
+                const double f = 2.0 * s / vnorm2;
+                for (int r = k; r < NB; ++r) A[r][q] -= f * vk[r];
+            }
+            double s = 0.0;
+            for (int r = k; r < NB; ++r) s += vk[r] * rhs[r];
+            const double f = 2.0 * s / vnorm2;
+            for (int r = k; r < NB; ++r) rhs[r] -= f * vk[r];
+        }
+        for (int q = k + 1; q < NB; ++q) norms[q] -= A[k][q] * A[k][q];
+        ++rank;
+    }
+    double z[NB];
+    for (int i = 0; i < NB; ++i) z[i] = 0.0;
+    for (int i = rank - 1; i >= 0; --i) {
+        double s = rhs[i];
+        for (int k = i + 1; k < rank; ++k) s -= A[i][k] * z[k];
+        z[i] = s / A[i][i];
+    }
+    for (int i = 0; i < NB; ++i) c[perm[i]] = z[i];
+    for (int i = 0; i < NB; ++i) c[i] /= D[i];
+    return 1;
+}
+
+// One block: reduce the block sums of a date in fixed order, then solve.
+template <int BASIS>
+__global__ void __launch_bounds__(32) lsm_solve_kernel(const double *__restrict__ block_sums, int nblocks, int d,
+                                                      double *__restrict__ coeffs, int *__restrict__ flags) {
+    constexpr int NB = BasisTraits<BASIS>::NB;
+    constexpr int NSUM = Sums<NB>::NSUM;
+    __shared__ double s_sum[NSUM];
+    if (threadIdx.x < NSUM) {
+        double t = 0.0;
+        for (int b = 0; b < nblocks; ++b) t += block_sums[static_cast<int64_t>(b) * NSUM + threadIdx.x];
+        s_sum[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double c[NB];
+        const int f = (BASIS == QK_LSM_LAGUERRE3) ? solve_reference<NB>(s_sum, c) : solve_scaled<NB>(s_sum, c);
+        for (int i = 0; i < kMaxCoef; ++i) coeffs[d * kMaxCoef + i] = i < NB ? c[i] : 0.0;
+        flags[d] = f;
+    }
+}
+
+// Exercise decision at date 0 (or the maturity payoff when there is a single
+// date), discount to t = 0, and per-block FP64 moments of the discounted cash
+// flows (ForwardBackwardMC.hpp:245-248 then OptionPricer::accumulate_batch_payoffs).
+template <class R, int BASIS>
+__global__ void __launch_bounds__(kLsmBlock) lsm_final_kernel(LsmArgs a, const R *__restrict__ slab_S,
+                                                             const R *__restrict__ slab_v, R *__restrict__ cf,
+                                                             int init, const double *__restrict__ coeffs,
+                                                             const double *__restrict__ centre,
+                                                             Moments *__restrict__ block_moments) {
+    constexpr int NB = BasisTraits<BASIS>::NB;
+    const R K = static_cast<R>(a.K);
+    const R disc = static_cast<R>(a.disc);
+    const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);
+    double cu[NB];
+    for (int i = 0; i < NB; ++i) cu[i] = init ? 0.0 : coeffs[i];
+    const double cx = centre[0], cv = centre[1];
+    const bool use_v = BASIS == QK_LSM_POLY_SV;
+    __shared__ Moments s_warp[kLsmBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Moments acc{0.0, 0.0, 0.0, 0.0};
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    const int64_t n_iter = (a.N + stride - 1) / stride;
+    for (int64_t it = 0; it < n_iter; ++it) {
+        const int64_t i = it * stride + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+        const bool active = i < a.N;
+        R val = R(0);
+        if (active) {
+            const R S = slab_S[i];
+            const R iv = lsm_intrinsic<R>(a.right, S, K);
+            R c;
+            if (init) {
+                c = iv;
+            } else {
+                c = cf[i];
+                const R disc_c = c * disc;
+                if (iv > R(0)) {
+                    const R v = use_v ? slab_v[i] : R(0);
+                    const double hold = continuation<R, BASIS>(cu, S, v, K, cx, cv);
+                    c = (static_cast<double>(iv) > hold) ? iv : disc_c;
+                } else {
+                    c = disc_c;
+                }
+            }
+            val = c * disc;  // t_1 -> 0 (LSMAmerican.hpp:401-405)
+            cf[i] = val;
+        }
+        const Moments wm = warp_moments(static_cast<double>(val), active, val > eps_payoff);
+        acc = chan_merge(acc, wm);
+    }
+    if (lane == 0) s_warp[warp] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        Moments m = lane < kLsmBlock / 32 ? s_warp[lane] : Moments{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) m = chan_merge(m, shfl_down_moments(m, off));
+        if (lane == 0) block_moments[blockIdx.x] = m;
+    }
+}
+
+// ---------------------------------------------------------------- host side
+namespace {
+
+#define QK_CUDA_LSM(call)                                                                            \
+    do {                                                                                             \
+        const cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? QK_ERR_OUT_OF_MEMORY : QK_ERR_CUDA,        \
+                        std::string("LSM: ") + #call + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+template <class R, int BASIS>
+cudaError_t enqueue_backward(cudaStream_t s, int grid, const LsmArgs &a, const R *S, const R *V, R *cf,
+                             double *coeffs, int *flags, const double *centre, double *block_sums,
+                             Moments *block_moments, int64_t *launches) {
+    const int D = a.n_dates;
+    if (D == 1) {
+        lsm_final_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, 1, coeffs, centre, block_moments);
+        ++*launches;
+        return cudaGetLastError();
+    }
+    lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre, block_sums);
+    ++*launches;
+    for (int d = D - 2; d >= 1; --d) {
+        lsm_solve_kernel<BASIS><<<1, 32, 0, s>>>(block_sums, grid, d, coeffs, flags);
+        lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, d, 0, d - 1, coeffs, centre, block_sums);
+        *launches += 2;
+    }
+    lsm_solve_kernel<BASIS><<<1, 32, 0, s>>>(block_sums, grid, 0, coeffs, flags);
+    lsm_final_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, 0, coeffs, centre, block_moments);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+void lsm_release(qk_handle *h) {
+    LsmArena &L = h->lsm;
+    L.slab_S.release();
+    L.slab_v.release();
+    L.cashflow.release();
+    L.block_sums.release();
+    L.coeffs.release();
+    L.task.release();
+    L.status.release();
+    h->h_lsm.release();
+    h->d_lsm_moments.release();
+}
+
+qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Moments> &moments) {
+    (void)moments;
+    plan.lsm_tasks.clear();
+    // task list
+    struct Job {
+        qk_contract b;
+        int contract, role;
+    };
+    std::vector<Job> jobs;
+    for (int i : plan.american)
+        for (int role : roles_for(plan.g_of(i), plan.norm[i].T)) {
+            qk_contract b = bumped(plan.norm[i], plan.g_of(i), role);
+            if (plain) b.precision = QK_FP64;
+            jobs.push_back({b, i, role});
+        }
+    const int grid = h->sm_count * 4;
+    const size_t nj = jobs.size();
+    qk_status st;
+    // sizes
+    size_t max_slab = 0, max_cf = 0;
+    int max_dates = 1;
+    for (const Job &j : jobs) {
+        const int D = j.b.lsm_dates > 0 ? j.b.lsm_dates : j.b.n_steps;
+        const int64_t ld = (j.b.n_paths + 3) / 4 * 4;
+        const size_t esz = j.b.precision == QK_FP32 ? 4 : 8;
+        max_slab = std::max(max_slab, static_cast<size_t>(D) * ld * esz);
+        max_cf = std::max(max_cf, static_cast<size_t>(ld) * esz);
+        max_dates = std::max(max_dates, D);
+    }
+    LsmArena &L = h->lsm;
+    if ((st = L.slab_S.ensure(max_slab)) != QK_OK) return st;
+    bool any_v = false;
+    for (const Job &j : jobs) any_v |= j.b.lsm_basis == QK_LSM_POLY_SV;
+    if (any_v && (st = L.slab_v.ensure(max_slab)) != QK_OK) return st;
+    if ((st = L.cashflow.ensure(max_cf)) != QK_OK) return st;
+    if ((st = L.block_sums.ensure(static_cast<size_t>(grid) * 64 * sizeof(double))) != QK_OK) return st;
+    if ((st = L.coeffs.ensure(static_cast<size_t>(max_dates) * kMaxCoef * sizeof(double) + 2 * max_dates * sizeof(double) * nj + 64)) != QK_OK) return st;
+    if ((st = L.status.ensure(static_cast<size_t>(max_dates) * sizeof(int))) != QK_OK) return st;
+    if ((st = L.task.ensure(nj * sizeof(TaskDev))) != QK_OK) return st;
+    if ((st = h->d_lsm_moments.ensure(nj * grid * sizeof(Moments))) != QK_OK) return st;
+    if ((st = h->h_lsm.ensure(nj * grid * sizeof(Moments))) != QK_OK) return st;
+    // descriptors and per-date centring constants (one upload, blocking)
+    std::vector<TaskDev> tasks(nj);
+    std::vector<double> centres;
+    std::vector<size_t> centre_off(nj);
+    for (size_t k = 0; k < nj; ++k) {
+        const qk_contract &b = jobs[k].b;
+        tasks[k] = make_task(b, 1);
+        const int D = b.lsm_dates > 0 ? b.lsm_dates : b.n_steps;
+        const int stride = b.n_steps / D;
+        const double dt = b.T / b.n_steps;
+        const double K = b.payoffs[0].strike;
+        centre_off[k] = centres.size();
+        for (int d = 0; d < D; ++d) {
+            const double t = (d + 1) * stride * dt;
+            // forward level of S/K and the mean of v_t: shifts that centre the regression basis
+            centres.push_back(b.S0 / K * std::exp((b.r - b.q) * t));
+            centres.push_back(b.theta + (b.v0 - b.theta) * std::exp(-b.kappa * t));
+        }
+    }
+    double *d_coeffs = static_cast<double *>(L.coeffs.ptr);
+    double *d_centre = d_coeffs + static_cast<size_t>(max_dates) * kMaxCoef;
+    QK_CUDA_LSM(cudaMemcpy(L.task.ptr, tasks.data(), nj * sizeof(TaskDev), cudaMemcpyHostToDevice));
+    QK_CUDA_LSM(cudaMemcpy(d_centre, centres.data(), centres.size() * sizeof(double), cudaMemcpyHostToDevice));
+    for (size_t k = 0; k < nj; ++k) {
+        const qk_contract &b = jobs[k].b;
+        const int D = b.lsm_dates > 0 ? b.lsm_dates : b.n_steps;
+        const int stride = b.n_steps / D;
+        const int64_t ld = (b.n_paths + 3) / 4 * 4;
+        const int prec = b.precision;
+        const bool use_v = b.lsm_basis == QK_LSM_POLY_SV;
+        // forward: exercise-date slabs
+        QK_CUDA_LSM(launch_slab_paths(prec, h->stream, static_cast<const TaskDev *>(L.task.ptr) + k, 0, b.n_paths,
+                                      stride, L.slab_S.ptr, use_v ? L.slab_v.ptr : nullptr, ld));
+        h->lsm_launches++;
+        LsmArgs a;
+        a.N = b.n_paths;
+        a.ld = ld;
+        a.right = b.payoffs[0].right;
+        a.n_dates = D;
+        a.K = b.payoffs[0].strike;
+        a.disc = std::exp(-b.r * stride * (b.T / b.n_steps));
+        Moments *bm = static_cast<Moments *>(h->d_lsm_moments.ptr) + k * grid;
+        const double *cen = d_centre + centre_off[k];
+        double *bs = static_cast<double *>(L.block_sums.ptr);
+        int *fl = static_cast<int *>(L.status.ptr);
+        cudaError_t e;
+        if (prec == QK_FP32) {
+            if (use_v)
+                e = enqueue_backward<float, QK_LSM_POLY_SV>(h->stream, grid, a, static_cast<const float *>(L.slab_S.ptr),
+                                                           static_cast<const float *>(L.slab_v.ptr),
+                                                           static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, bm,
+                                                           &h->lsm_launches);
+            else
+                e = enqueue_backward<float, QK_LSM_LAGUERRE3>(h->stream, grid, a, static_cast<const float *>(L.slab_S.ptr),
+                                                             nullptr, static_cast<float *>(L.cashflow.ptr), d_coeffs, fl,
+                                                             cen, bs, bm, &h->lsm_launches);
+        } else {
+            if (use_v)
+                e = enqueue_backward<double, QK_LSM_POLY_SV>(h->stream, grid, a, static_cast<const double *>(L.slab_S.ptr),
+                                                            static_cast<const double *>(L.slab_v.ptr),
+                                                            static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen, bs,
+                                                            bm, &h->lsm_launches);
+            else
+                e = enqueue_backward<double, QK_LSM_LAGUERRE3>(h->stream, grid, a,
+                                                              static_cast<const double *>(L.slab_S.ptr), nullptr,
+                                                              static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen,
+                                                              bs, bm, &h->lsm_launches);
+        }
+        if (e != cudaSuccess) return fail(QK_ERR_CUDA, std::string("LSM launch: ") + cudaGetErrorString(e));
+        LsmTaskInfo info;
+        info.contract = jobs[k].contract;
+        info.role = jobs[k].role;
+        info.grid = grid;
+        info.n_paths = b.n_paths;
+        // immediate exercise value today at S0 (LSMAmerican.hpp:410-418)
+        const double K = b.payoffs[0].strike;
+        info.intrinsic0 = b.payoffs[0].right == QK_CALL ? std::max(b.S0 - K, 0.0) : std::max(K - b.S0, 0.0);
+        info.eps = prec == QK_FP32 ? 1e-6 : 1e-12;
+        plan.lsm_tasks.push_back(info);
+        plan.lsm_path_steps += static_cast<double>(b.n_paths) * b.n_steps;
+    }
+    QK_CUDA_LSM(cudaMemcpyAsync(h->h_lsm.ptr, h->d_lsm_moments.ptr, nj * grid * sizeof(Moments),
+                                cudaMemcpyDeviceToHost, h->stream));
+    return QK_OK;
+}
+
+void assemble_lsm_results(qk_handle *h, const Plan &plan, const std::vector<Moments> &, qk_result *out) {
+    const Moments *hm = static_cast<const Moments *>(h->h_lsm.ptr);
+    // per task merged moments after the day-zero decision
+    std::vector<double> price(plan.lsm_tasks.size()), se(plan.lsm_tasks.size()), itm(plan.lsm_tasks.size());
+    for (size_t k = 0; k < plan.lsm_tasks.size(); ++k) {
+        const LsmTaskInfo &info = plan.lsm_tasks[k];
+        Moments m{0.0, 0.0, 0.0, 0.0};
+        for (int b = 0; b < info.grid; ++b) {
+            const Moments &o = hm[k * info.grid + b];
+            const double n = m.n + o.n;
+            if (o.n <= 0.0) continue;
+            if (m.n <= 0.0) {
+                m = o;
+                continue;
+            }
+            const double d = o.mean - m.mean;
+            m.mean += d * (o.n / n);
+            m.m2 += o.m2 + d * d * (m.n * o.n / n);
+            m.itm += o.itm;
+            m.n = n;
+        }
+        // LSMEngine::apply_final_discount: exercise today if intrinsic(S0) beats the mean
+        if (info.intrinsic0 > m.mean) {
+            m.mean = info.intrinsic0;
+            m.m2 = 0.0;
+            m.itm = info.intrinsic0 > info.eps ? m.n : 0.0;
+        }
+        const double scale = plan.scale[info.contract];
+        const double N = m.n;
+        price[k] = m.mean * scale;
+        se[k] = N > 1.0 ? std::sqrt(m.m2 / (N - 1.0) / N) * scale : 0.0;
+        itm[k] = N > 0.0 ? m.itm / N : 0.0;
+    }
+    for (int i : plan.american) {
+        const qk_greeks *g = plan.g_of(i);
+        qk_result &r = out[i];
+        std::memset(&r, 0, sizeof(r));
+        const qk_contract &n = plan.norm[i];
+        r.status = QK_OK;
+        r.n_payoffs = 1;
+        r.n_paths = n.n_paths;
+        auto find = [&](int role) -> int {
+            for (size_t k = 0; k < plan.lsm_tasks.size(); ++k)
+                if (plan.lsm_tasks[k].contract == i && plan.lsm_tasks[k].role == role) return static_cast<int>(k);
+            return -1;
+        };
+        auto p_of = [&](int role) {
+            const int k = find(role);
+            return k >= 0 ? price[k] : 0.0;
+        };
+        for (size_t k = 0; k < plan.lsm_tasks.size(); ++k)
+            if (plan.lsm_tasks[k].contract == i)
+                r.path_steps += static_cast<double>(plan.lsm_tasks[k].n_paths) * n.n_steps;
+        const int k0 = find(0);
+        qk_payoff_result &pr = r.p[0];
+        pr.price = price[k0];
+        pr.std_error = se[k0];
+        pr.prob_itm = itm[k0];
+        if (!g) continue;
+        const double p0 = pr.price;
+        const double h_S_real = (n.normalize ? plan.scale[i] : n.S0) * g->bump_S_rel;
+        const double h_vol = g->vega_mode == 1 ? n.v0 * g->bump_vol : g->bump_vol;
+        if (g->mask & QK_GREEK_DELTA_GAMMA) {
+            const double pu = p_of(1), pd = p_of(2);
+            pr.delta = (pu - pd) / (2.0 * h_S_real);
+            pr.gamma = (pu - 2.0 * p0 + pd) / (h_S_real * h_S_real);
+        }
+        if (g->mask & QK_GREEK_VEGA_VOMMA) {
+            const double pu = p_of(3), pd = p_of(4);
+            pr.vega = (pu - pd) / (2.0 * h_vol);
+            pr.vomma = (pu - 2.0 * p0 + pd) / (h_vol * h_vol);
+        }
+        if (g->mask & QK_GREEK_RHO) pr.rho = (p_of(5) - p_of(6)) / (2.0 * g->bump_r_abs);
+        if (g->mask & QK_GREEK_THETA) pr.theta = n.T > g->bump_T_abs ? (p_of(7) - p0) / g->bump_T_abs : 0.0;
+        if (g->mask & QK_GREEK_VANNA)
+            pr.vanna = (p_of(8) - p_of(9) - p_of(10) + p_of(11)) / (4.0 * h_S_real * h_vol);
+    }
+}
+
+}  // namespace qk

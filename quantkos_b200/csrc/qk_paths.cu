@@ -1,0 +1,382 @@
+// Path-generation kernels (sm_100a): the fused path + payoff pricing kernel
+// (persistent, fed by a device queue of (task, path-block) tiles), the per-task
+// FP64 merge, the exercise-date slab writer used by Longstaff-Schwartz and by
+// the path dump, and the fed-draw parity trace.
+#include <cuda_runtime.h>
+
+#include "qk_device.cuh"
+#include "qk_kernels.h"
+
+namespace qk {
+
+// ----------------------------------------------------------------------------
+// One path of one task.  Mirrors MarkovianIntegrationKernel::operator()
+// (include/core/schemes/markovian/MSolver.hpp:98-130): start at (S0, v0), step
+// n_steps times, track the running average / max / min after every step.
+// SINK is called after each step with (step index, S, v).
+// ----------------------------------------------------------------------------
+template <class R>
+struct PathState {
+    R S, v;
+    double ssum;
+    R smax, smin;
+};
+
+struct NoSink {
+    template <class R>
+    __device__ __forceinline__ void operator()(int, R, R) const {}
+};
+
+template <class R>
+struct SlabSink {
+    R *slab_S;
+    R *slab_v;
+    int64_t ld;     // leading dimension (paths per slab row)
+    int64_t col;    // this path's column
+    int stride;     // steps between stored dates
+    __device__ __forceinline__ void operator()(int n, R S, R v) const {
+        const int np1 = n + 1;
+        if (np1 % stride == 0) {
+            const int64_t row = np1 / stride - 1;
+            slab_S[row * ld + col] = S;
+            if (slab_v) slab_v[row * ld + col] = v;
+        }
+    }
+};
+
+template <class R>
+__device__ __forceinline__ void track(PathState<R> &st) {
+    st.ssum += static_cast<double>(st.S);
+    st.smax = rmax(st.smax, st.S);
+    st.smin = rmin(st.smin, st.S);
+}
+
+template <class R, int MODEL, int SCHEME, class Sink>
+__device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0, int n_steps, uint32_t k0,
+                                              uint32_t k1, uint32_t path, uint32_t stream, PathState<R> &st,
+                                              const Sink &sink) {
+    st.S = S0;
+    st.v = v0;
+    st.ssum = 0.0;
+    st.smax = S0;
+    st.smin = S0;
+    if constexpr (MODEL == kHeston) {
+        int n = 0;
+        for (; n + 1 < n_steps; n += 2) {
+            const U4 w = philox4x32_10(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u}, k0, k1);
+            R z1, z2;
+            Math<R>::box_muller(w.x, w.y, z1, z2);
+            heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
+            track(st);
+            sink(n, st.S, st.v);
+            Math<R>::box_muller(w.z, w.w, z1, z2);
+            heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
+            track(st);
+            sink(n + 1, st.S, st.v);
+        }
+        if (n < n_steps) {
+            const U4 w = philox4x32_10(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u}, k0, k1);
+            R z1, z2;
+            Math<R>::box_muller(w.x, w.y, z1, z2);
+            heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
+            track(st);
+            sink(n, st.S, st.v);
+        }
+    } else {
+        for (int n = 0; n < n_steps; ++n) {
+            PhiloxBatesStep<R> d;
+            d.k0 = k0;
+            d.k1 = k1;
+            d.path = path;
+            d.stream = stream;
+            d.step = n;
+            d.w0 = philox4x32_10(U4{static_cast<uint32_t>(n), path, stream, 0u}, k0, k1);
+            d.used = 0;
+            d.domain = 0;
+            evolve_step<R, kBates, SCHEME>(p, st.S, st.v, d);
+            track(st);
+            sink(n, st.S, st.v);
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ const StepConst<R> &task_const(const TaskDev &t);
+template <>
+__device__ __forceinline__ const StepConst<float> &task_const<float>(const TaskDev &t) { return t.cf; }
+template <>
+__device__ __forceinline__ const StepConst<double> &task_const<double>(const TaskDev &t) { return t.cd; }
+
+template <class R, class Sink>
+__device__ __forceinline__ void simulate_dispatch(const TaskDev &t, const StepConst<R> &p, uint32_t path,
+                                                  PathState<R> &st, const Sink &sink) {
+    const R S0 = static_cast<R>(t.S0);
+    const R v0 = static_cast<R>(t.v0);
+    switch (t.model * 3 + t.scheme) {
+        case 0: simulate_path<R, kHeston, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+        case 1: simulate_path<R, kHeston, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+        case 2: simulate_path<R, kHeston, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+        case 3: simulate_path<R, kBates, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+        case 4: simulate_path<R, kBates, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+        default: simulate_path<R, kBates, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Fused pricing kernel.  Persistent: each block pops queue slots from a device
+// cursor; slot q belongs to the task whose tile range [tile_begin, tile_begin +
+// n_tiles) holds it (binary search over the task prefix, tasks ordered by the
+// host's schedule).  A tile is ppt rounds of one path per thread; every
+// requested payoff leg is evaluated in registers and folded into per-warp FP64
+// moments (n, mean, M2, #ITM), then into one record per tile and leg.  The
+// reference writes payoffs to memory and reduces them in two more passes
+// (OptionPricer.hpp:123-193); here nothing per path leaves registers.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int n_tasks, int64_t q) {
+    int lo = 0, hi = n_tasks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kPathBlock) price_tiles_kernel(const TaskDev *__restrict__ tasks,
+                                                                const int64_t *__restrict__ prefix, int32_t n_tasks,
+                                                                int64_t slot_begin, int64_t slot_end,
+                                                                unsigned long long *__restrict__ cursor,
+                                                                Moments *__restrict__ partials) {
+    __shared__ int64_t s_slot;
+    __shared__ Moments s_warp[QK_MAX_PAYOFFS][kPathBlock / 32];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);  // OptionPricer.hpp:316
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int64_t q = slot_begin + static_cast<int64_t>(atomicAdd(cursor, 1ull));
+            s_slot = q < slot_end ? q : -1;
+        }
+        __syncthreads();
+        const int64_t slot = s_slot;
+        __syncthreads();
+        if (slot < 0) return;
+
+        const int ti = find_task(prefix, n_tasks, slot);
+        const TaskDev &t = tasks[ti];
+        const int64_t tile = slot - t.tile_begin;
+        const StepConst<R> p = task_const<R>(t);
+        const int np = t.n_payoffs;
+        const int ppt = t.ppt;
+        const int64_t tile_first = tile * static_cast<int64_t>(kPathBlock) * ppt;
+        // lane 0 of each warp keeps the warp's running moments in shared memory
+        if (lane == 0)
+            for (int k = 0; k < np; ++k) s_warp[k][warp] = Moments{0.0, 0.0, 0.0, 0.0};
+
+        for (int j = 0; j < ppt; ++j) {
+            const int64_t path = tile_first + static_cast<int64_t>(j) * kPathBlock + threadIdx.x;
+            const bool active = path < t.n_paths;
+            if (__syncthreads_or(active) == 0) break;
+            PathState<R> st;
+            if (active) {
+                simulate_dispatch<R>(t, p, static_cast<uint32_t>(path), st, NoSink{});
+            } else {
+                st.S = st.smax = st.smin = R(0);
+                st.ssum = 0.0;
+            }
+            for (int k = 0; k < np; ++k) {
+                const PayoffSpec ps = t.pay[k];
+                const R x = active ? final_payoff<R>(ps, st.S, st.ssum, st.smax, st.smin, t.n_steps) : R(0);
+                const Moments wm = warp_moments(static_cast<double>(x), active, x > eps_payoff);
+                if (lane == 0) s_warp[k][warp] = chan_merge(s_warp[k][warp], wm);
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int k = 0; k < np; ++k) {
+                Moments m = lane < kPathBlock / 32 ? s_warp[k][lane] : Moments{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    const Moments o = shfl_down_moments(m, off);
+                    m = chan_merge(m, o);
+                }
+                if (lane == 0) partials[t.partial_base + tile * np + k] = m;
+            }
+        }
+    }
+}
+
+// Per task and leg: merge the task's tile moments (Chan updates, strided per
+// thread, then a fixed-shape tree), deterministic for a given tile plan.
+__global__ void __launch_bounds__(256) merge_tasks_kernel(const TaskDev *__restrict__ tasks,
+                                                          const Moments *__restrict__ partials,
+                                                          TaskMoments *__restrict__ out) {
+    __shared__ Moments s[256];
+    const TaskDev &t = tasks[blockIdx.x];
+    for (int k = 0; k < t.n_payoffs; ++k) {
+        Moments acc{0.0, 0.0, 0.0, 0.0};
+        for (int i = threadIdx.x; i < t.n_tiles; i += blockDim.x)
+            acc = chan_merge(acc, partials[t.partial_base + static_cast<int64_t>(i) * t.n_payoffs + k]);
+        s[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (static_cast<int>(threadIdx.x) < w) s[threadIdx.x] = chan_merge(s[threadIdx.x], s[threadIdx.x + w]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const Moments m = s[0];
+            out[static_cast<int64_t>(blockIdx.x) * QK_MAX_PAYOFFS + k] = m;
+        }
+        __syncthreads();
+    }
+}
+
+// Exercise-date slabs (LSM) / full path dump: one path per thread, S (and v)
+// after every `stride`-th step stored as SoA rows slab[date][path].
+template <class R>
+__global__ void __launch_bounds__(kPathBlock) slab_paths_kernel(const TaskDev *__restrict__ task, int64_t first_path,
+                                                               int64_t count, int stride, R *__restrict__ slab_S,
+                                                               R *__restrict__ slab_v, int64_t ld) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const TaskDev &t = *task;
+    const StepConst<R> p = task_const<R>(t);
+    SlabSink<R> sink{slab_S, slab_v, ld, i, stride};
+    PathState<R> st;
+    simulate_dispatch<R>(t, p, static_cast<uint32_t>(first_path + i), st, sink);
+}
+
+// Per-path payoff of leg 0 (undiscounted, normalised units), for the payoff
+// distribution analysis (OptionPricer.hpp:340-360 sorts every path's payoff).
+template <class R>
+__global__ void __launch_bounds__(kPathBlock) payoff_paths_kernel(const TaskDev *__restrict__ task, int64_t count,
+                                                                 double *__restrict__ out) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const TaskDev &t = *task;
+    const StepConst<R> p = task_const<R>(t);
+    PathState<R> st;
+    simulate_dispatch<R>(t, p, static_cast<uint32_t>(i), st, NoSink{});
+    out[i] = static_cast<double>(final_payoff<R>(t.pay[0], st.S, st.ssum, st.smax, st.smin, t.n_steps));
+}
+
+// Fed-draw trace of the step functions (one thread).
+template <class R>
+__global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double *__restrict__ z,
+                                  const double *__restrict__ u, int umax, int n, double *__restrict__ S_out,
+                                  double *__restrict__ v_out, int *__restrict__ status) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const TaskDev &t = *task;
+    const StepConst<R> p = task_const<R>(t);
+    R S = static_cast<R>(t.S0);
+    R v = static_cast<R>(t.v0);
+    for (int i = 0; i < n; ++i) {
+        FedStep<R> d{z + 3 * static_cast<int64_t>(i), u + static_cast<int64_t>(umax) * i, umax, 0, 0};
+        switch (t.model * 3 + t.scheme) {
+            case 0: evolve_step<R, kHeston, kEuler>(p, S, v, d); break;
+            case 1: evolve_step<R, kHeston, kMilstein>(p, S, v, d); break;
+            case 2: evolve_step<R, kHeston, kQE>(p, S, v, d); break;
+            case 3: evolve_step<R, kBates, kEuler>(p, S, v, d); break;
+            case 4: evolve_step<R, kBates, kMilstein>(p, S, v, d); break;
+            default: evolve_step<R, kBates, kQE>(p, S, v, d); break;
+        }
+        if (d.overflow) {
+            *status = 1;
+            return;
+        }
+        S_out[i] = static_cast<double>(S);
+        v_out[i] = static_cast<double>(v);
+    }
+    *status = 0;
+}
+
+// ----------------------------------------------------------------------------
+// Launchers
+// ----------------------------------------------------------------------------
+cudaError_t launch_price_tiles(int precision, int grid, cudaStream_t s, const TaskDev *tasks, const int64_t *prefix,
+                               int32_t n_tasks, int64_t slot_begin, int64_t slot_end, unsigned long long *cursor,
+                               Moments *partials) {
+    if (precision == QK_FP32)
+        price_tiles_kernel<float><<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials);
+    else
+        price_tiles_kernel<double><<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
+                               TaskMoments *out) {
+    merge_tasks_kernel<<<n_tasks, 256, 0, s>>>(tasks, partials, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slab_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t first_path, int64_t count,
+                              int stride, void *slab_S, void *slab_v, int64_t ld) {
+    const int64_t blocks = (count + kPathBlock - 1) / kPathBlock;
+    if (precision == QK_FP32)
+        slab_paths_kernel<float><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
+            task, first_path, count, stride, static_cast<float *>(slab_S), static_cast<float *>(slab_v), ld);
+    else
+        slab_paths_kernel<double><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
+            task, first_path, count, stride, static_cast<double *>(slab_S), static_cast<double *>(slab_v), ld);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
+                              int umax, int n, double *S_out, double *v_out, int *status) {
+    if (precision == QK_FP32)
+        step_trace_kernel<float><<<1, 1, 0, s>>>(task, z, u, umax, n, S_out, v_out, status);
+    else
+        step_trace_kernel<double><<<1, 1, 0, s>>>(task, z, u, umax, n, S_out, v_out, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out) {
+    const int64_t blocks = (count + kPathBlock - 1) / kPathBlock;
+    if (precision == QK_FP32)
+        payoff_paths_kernel<float><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(task, count, out);
+    else
+        payoff_paths_kernel<double><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(task, count, out);
+    return cudaGetLastError();
+}
+
+// SFU throughput probe: 8 independent chains x = 2^(-x) per thread (ex2.approx.ftz in
+// hand-written PTX), so every iteration issues 8 MUFU.EX2 with no other dependency.
+__global__ void __launch_bounds__(256) sfu_probe_kernel(float *sink, int iters) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = 0.001f * (threadIdx.x + 1) + 0.1f * k;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) asm volatile("ex2.approx.ftz.f32 %0, %1;" : "=f"(x[k]) : "f"(-x[k]));
+    }
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc += x[k];
+    if (acc == 12345.0f) sink[threadIdx.x] = acc;  // keeps the chains live
+}
+
+cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
+                             double *ops) {
+    const int blocks = sm_count * 8, threads = 256, iters = 4096;
+    sfu_probe_kernel<<<blocks, threads, 0, s>>>(sink, 64);  // warm-up
+    cudaEventRecord(e0, s);
+    sfu_probe_kernel<<<blocks, threads, 0, s>>>(sink, iters);
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) return e;
+    e = cudaEventElapsedTime(ms, e0, e1);
+    *ops = static_cast<double>(blocks) * threads * iters * 8.0;
+    return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+int price_tiles_max_blocks_per_sm(int precision) {
+    int nb = 0;
+    if (precision == QK_FP32)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_tiles_kernel<float>, kPathBlock, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_tiles_kernel<double>, kPathBlock, 0);
+    return nb > 0 ? nb : 1;
+}
+
+}  // namespace qk

@@ -1,0 +1,254 @@
+// Continuous-batching request loop.
+//
+// Requests are queued by qk_serve_submit (any thread).  Lanes — host threads,
+// each with its own handle and CUDA stream on the same device — take whatever
+// has arrived, in arrival order, as long as the HBM the requests need fits in
+// what the budget has free, and price it as one batch (one persistent launch
+// plus the LSM sweeps of its American contracts).  While one lane's batch is on
+// the GPU, the next lane admits the requests that arrived meanwhile, so their
+// work overlaps on the device; memory is returned to the budget as each batch
+// completes.  A request larger than the whole budget is rejected
+// (QK_ERR_CAPACITY).  The reference has no serving layer (one contract per
+// process run, include/core/engine/Distpatcher.hpp:78-83).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "qk_engine.h"
+#include "qk_host.h"
+#include "qk_kernels.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    int64_t ticket;
+    qk_contract c;
+    qk_greeks g;
+    size_t bytes;
+    Clock::time_point t_submit;
+};
+
+struct Finished {
+    qk_result r;
+    qk_status status;
+    double latency_ms;
+};
+
+// HBM a request holds while it is being priced: LSM slabs and cash flows for
+// American contracts, per-tile moment records and descriptors otherwise.
+size_t footprint(const qk_contract &c, const qk_greeks &g) {
+    const size_t roles = qk::roles_for(g.mask ? &g : nullptr, c.T).size();
+    const size_t esz = c.precision == QK_FP32 ? 4 : 8;
+    size_t bytes = roles * (sizeof(qk::TaskDev) + 64);
+    if (c.payoffs[0].type == QK_AMERICAN) {
+        const size_t D = c.lsm_dates > 0 ? c.lsm_dates : c.n_steps;
+        const size_t ld = (static_cast<size_t>(c.n_paths) + 3) / 4 * 4;
+        const size_t slabs = c.lsm_basis == QK_LSM_POLY_SV ? 2 : 1;
+        bytes += D * ld * esz * slabs + ld * esz;  // slabs are reused across the bumps of one request
+    } else {
+        const size_t tiles = (static_cast<size_t>(c.n_paths) + qk::kPathBlock - 1) / qk::kPathBlock;
+        bytes += roles * tiles * c.n_payoffs * sizeof(qk::Moments);
+    }
+    return bytes;
+}
+
+}  // namespace
+
+struct qk_server {
+    int device = 0;
+    size_t budget = 0, in_use = 0;
+    int max_batch = 256;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request> queue;
+    std::unordered_map<int64_t, Finished> done;
+    int64_t next_ticket = 1;
+    bool stop = false;
+    std::vector<std::thread> lanes;
+    std::vector<qk_handle *> handles;
+    // statistics
+    std::vector<double> latencies;
+    int64_t submitted = 0, completed = 0, rejected = 0, batches = 0;
+    double path_steps = 0.0, busy_s = 0.0;
+    bool have_first = false;
+    Clock::time_point t_first, t_last;
+};
+
+static void lane_loop(qk_server *s, qk_handle *h) {
+    std::vector<Request> batch;
+    std::vector<qk_contract> cs;
+    std::vector<qk_greeks> gs;
+    std::vector<qk_result> rs;
+    for (;;) {
+        batch.clear();
+        size_t bytes = 0;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            for (;;) {
+                if (s->stop && s->queue.empty()) return;
+                while (!s->queue.empty() && static_cast<int>(batch.size()) < s->max_batch &&
+                       s->in_use + bytes + s->queue.front().bytes <= s->budget) {
+                    bytes += s->queue.front().bytes;
+                    batch.push_back(s->queue.front());
+                    s->queue.pop_front();
+                }
+                if (!batch.empty()) break;
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            }
+            s->in_use += bytes;
+        }
+        cs.resize(batch.size());
+        gs.resize(batch.size());
+        rs.resize(batch.size());
+        for (size_t i = 0; i < batch.size(); ++i) {
+            cs[i] = batch[i].c;
+            gs[i] = batch[i].g;
+        }
+        const auto t0 = Clock::now();
+        const qk_status st = qk::price_contracts(h, cs.data(), static_cast<int32_t>(cs.size()), gs.data(), rs.data(), false);
+        const auto t1 = Clock::now();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->in_use -= bytes;
+            s->batches++;
+            s->busy_s += std::chrono::duration<double>(t1 - t0).count();
+            for (size_t i = 0; i < batch.size(); ++i) {
+                Finished f;
+                f.status = st;
+                f.r = rs[i];
+                if (st != QK_OK) f.r.status = st;
+                f.latency_ms = std::chrono::duration<double, std::milli>(t1 - batch[i].t_submit).count();
+                s->latencies.push_back(f.latency_ms);
+                s->completed++;
+                if (st == QK_OK) s->path_steps += rs[i].path_steps;
+                s->done[batch[i].ticket] = f;
+            }
+            s->t_last = t1;
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+}
+
+extern "C" {
+
+qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch, qk_server **out) {
+    if (!h || !out) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    *out = nullptr;
+    if (cudaSetDevice(h->device) != cudaSuccess) return qk::fail(QK_ERR_CUDA, "cudaSetDevice failed");
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return qk::fail(QK_ERR_CUDA, "cudaMemGetInfo failed");
+    qk_server *s = new qk_server();
+    s->device = h->device;
+    s->budget = hbm_budget_mib > 0 ? static_cast<size_t>(hbm_budget_mib) << 20 : static_cast<size_t>(free_b * 0.8);
+    s->max_batch = max_batch > 0 ? max_batch : 256;
+    constexpr int kLanes = 2;
+    for (int i = 0; i < kLanes; ++i) {
+        qk_handle *lh = nullptr;
+        const qk_status st = qk_create(h->device, &lh);
+        if (st != QK_OK) {
+            for (qk_handle *x : s->handles) qk_destroy(x);
+            delete s;
+            return st;
+        }
+        s->handles.push_back(lh);
+    }
+    for (qk_handle *lh : s->handles) s->lanes.emplace_back(lane_loop, s, lh);
+    *out = s;
+    return QK_OK;
+}
+
+qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g, int64_t *ticket) {
+    if (!s || !c || !ticket) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    const qk_status v = qk::validate_contract(*c, g);
+    if (v != QK_OK) return v;
+    Request r;
+    r.c = *c;
+    if (g) r.g = *g;
+    else std::memset(&r.g, 0, sizeof(r.g));
+    r.bytes = footprint(r.c, r.g);
+    r.t_submit = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return qk::fail(QK_ERR_STATE, "server stopped");
+    if (!s->have_first) {
+        s->have_first = true;
+        s->t_first = r.t_submit;
+    }
+    s->submitted++;
+    if (r.bytes > s->budget) {
+        s->rejected++;
+        return qk::fail(QK_ERR_CAPACITY, "request needs more HBM than the admission budget");
+    }
+    r.ticket = s->next_ticket++;
+    *ticket = r.ticket;
+    s->queue.push_back(r);
+    s->cv_work.notify_one();
+    return QK_OK;
+}
+
+qk_status qk_serve_poll(qk_server *s, int64_t ticket, int32_t wait_ms, int32_t *done, qk_result *out) {
+    if (!s || !done) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    *done = 0;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (ticket <= 0 || ticket >= s->next_ticket) return qk::fail(QK_ERR_STATE, "unknown ticket");
+    auto ready = [&] { return s->done.count(ticket) > 0; };
+    if (!ready() && wait_ms > 0) s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), ready);
+    auto it = s->done.find(ticket);
+    if (it == s->done.end()) return QK_OK;
+    *done = 1;
+    if (out) *out = it->second.r;
+    const qk_status st = it->second.status;
+    s->done.erase(it);
+    return st;
+}
+
+qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out) {
+    if (!s || !out) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::memset(out, 0, sizeof(*out));
+    out->submitted = s->submitted;
+    out->completed = s->completed;
+    out->rejected = s->rejected;
+    out->batches = s->batches;
+    out->busy_s = s->busy_s;
+    if (!s->latencies.empty()) {
+        std::vector<double> l = s->latencies;
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double p) { return l[std::min(l.size() - 1, static_cast<size_t>(p * (l.size() - 1) + 0.5))]; };
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        out->p999_ms = pct(0.999);
+        out->max_ms = l.back();
+        const double span = std::chrono::duration<double>(s->t_last - s->t_first).count();
+        if (span > 0.0) {
+            out->contracts_per_s = static_cast<double>(s->completed) / span;
+            out->path_steps_per_s = s->path_steps / span;
+        }
+    }
+    return QK_OK;
+}
+
+qk_status qk_serve_stop(qk_server *s) {
+    if (!s) return QK_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->lanes) t.join();
+    for (qk_handle *h : s->handles) qk_destroy(h);
+    delete s;
+    return QK_OK;
+}
+
+}  // extern "C"
