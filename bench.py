@@ -48,11 +48,14 @@ L2_FLUSH_BYTES = 256 << 20
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample-paths", type=int, default=1 << 16)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--paths", type=int, default=N_PATHS,
+                    help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
     return ap.parse_args()
 
 
@@ -80,7 +83,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
@@ -203,8 +206,8 @@ def main() -> None:
     h = qk.Handle(local_rank)
     ext = torch.cuda.ExternalStream(h.stream())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    contract = workload_contract(qk, rank)
-    path_steps = float(N_PATHS) * N_STEPS
+    contract = workload_contract(qk, rank, n_paths=args.paths)
+    path_steps = float(args.paths) * N_STEPS
 
     # ---- value: descriptors resident in HBM, K device-timed pricings
     prep = qk.PreparedBatch([contract], None, h)
@@ -275,7 +278,7 @@ def main() -> None:
     # ---- plain FP64 drop-in on the same workload (equal paths => equal standard error)
     plain = None
     if not args.no_plain:
-        c64 = workload_contract(qk, rank, qk.FP64)
+        c64 = workload_contract(qk, rank, qk.FP64, args.paths)
         qk.price_plain(c64, None, h)
         r64 = qk.price_plain(c64, None, h)
         t64 = h.last_timing()
@@ -293,7 +296,7 @@ def main() -> None:
     clocks = sampler.summary(peaks.get("sm_max_mhz", 1965.0))
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.skip_cpu:
         try:
             cpu = {k: v for k, v in cpu_reference_rate(args.cpu_sample_paths).items() if k != "seconds"}
         except Exception as e:  # the baseline is reported, never required
@@ -304,7 +307,8 @@ def main() -> None:
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_paths": N_PATHS, "n_steps": N_STEPS, "payoff_legs": 5,
+            "config": {"workload": WORKLOAD if args.paths == N_PATHS else f"{WORKLOAD} (reduced to {args.paths} paths)",
+                       "n_paths": args.paths, "n_steps": N_STEPS, "payoff_legs": 5,
                        "parallelism": f"contract-per-gpu x{world}", "l2": "flushed between timed steps (256 MiB write)",
                        "contracts_per_s": world / (ms_per_step * 1e-3)},
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -144,7 +144,7 @@ typedef struct {
     int umax, used, overflow;
     /* philox */
     uint32_t k0, k1, path, stream, step;
-    uint32_t w0[4];
+    uint32_t w_first; /* word of the step's first Poisson uniform */
     uint32_t wx[4];
     int domain;
 } Draws;
@@ -154,14 +154,16 @@ static double draw_uniform_d(Draws *d, int as_float) {
         if (d->used >= d->umax) { d->overflow = 1; return 0.0; }
         return d->u[d->used++];
     }
+    /* Philox layout of the Poisson uniforms of step n (engine's draw layout):
+       1st: domain 2, block n/4, word n%4; 2nd, 3rd: domain 1, block n, words z, w;
+       k-th (k >= 4, 1-based): domain 3 + (k-4)/4, block n, word (k-4)%4. */
     const int k = d->used++;
     uint32_t word;
-    if (k == 0) word = d->w0[2];
-    else if (k == 1) word = d->w0[3];
+    if (k == 0) word = d->w_first;
     else {
-        const int dom = (k < 4) ? 1 : 2 + (k - 4) / 4;
+        const int dom = (k < 3) ? 1 : 3 + (k - 3) / 4;
         if (d->domain != dom) { philox_block(d->step, d->path, d->stream, (uint32_t)dom, d->k0, d->k1, d->wx); d->domain = dom; }
-        const int slot = (k < 4) ? k : ((k - 4) & 3);
+        const int slot = (k < 3) ? k + 1 : ((k - 3) & 3);
         word = d->wx[slot];
     }
     return as_float ? (double)u01f(word) : u01d(word);
@@ -366,20 +368,18 @@ static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_
     float Sf = (float)c->S0, vf = (float)c->v0;
     double ssum = 0.0, smax = fp32 ? (double)Sf : S, smin = smax;
     float smaxf = Sf, sminf = Sf;
-    uint32_t w[4] = {0, 0, 0, 0};
+    uint32_t w[4] = {0, 0, 0, 0}, wp[4] = {0, 0, 0, 0};
     for (int n = 0; n < c->n_steps; ++n) {
         Draws d;
         memset(&d, 0, sizeof(d));
         d.k0 = k0; d.k1 = k1; d.path = path; d.stream = stream; d.step = (uint32_t)n;
-        uint32_t wa, wb;
-        if (c->model == QK_HESTON) {
-            if ((n & 1) == 0) philox_block((uint32_t)(n >> 1), path, stream, 0u, k0, k1, w);
-            wa = (n & 1) ? w[2] : w[0];
-            wb = (n & 1) ? w[3] : w[1];
-        } else {
-            philox_block((uint32_t)n, path, stream, 0u, k0, k1, d.w0);
-            wa = d.w0[0];
-            wb = d.w0[1];
+        /* normal pair of step n: domain 0, block n/2, words (x,y) for even n, (z,w) for odd n */
+        if ((n & 1) == 0) philox_block((uint32_t)(n >> 1), path, stream, 0u, k0, k1, w);
+        const uint32_t wa = (n & 1) ? w[2] : w[0];
+        const uint32_t wb = (n & 1) ? w[3] : w[1];
+        if (c->model == QK_BATES) {
+            if ((n & 3) == 0) philox_block((uint32_t)(n >> 2), path, stream, 2u, k0, k1, wp);
+            d.w_first = wp[n & 3];
         }
         if (fp32) {
             float z1, z2;

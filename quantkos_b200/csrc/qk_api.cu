@@ -210,7 +210,11 @@ TaskDev make_task(const qk_contract &b, int ppt) {
     t.stream = static_cast<uint32_t>(b.stream);
     t.n_paths = b.n_paths;
     t.ppt = ppt;
-    const int64_t tile_paths = static_cast<int64_t>(kPathBlock) * ppt;
+    // FP32 jump test on the raw word: u01(w) = ((w >> 9) + 1/2) 2^-23 >= L  <=>  (w >> 9) >= kmin
+    const float Lf = t.cf.exp_m_lambda_dt;
+    const double kd = std::ceil(static_cast<double>(Lf) * 8388608.0 - 0.5);
+    t.jump_kmin = static_cast<uint32_t>(std::min(std::max(kd, 0.0), 8388608.0));
+    const int64_t tile_paths = static_cast<int64_t>(kWarpTilePaths) * ppt;
     t.n_tiles = static_cast<int32_t>((b.n_paths + tile_paths - 1) / tile_paths);
     for (int k = 0; k < b.n_payoffs; ++k) {
         t.pay[k].type = b.payoffs[k].type;
@@ -230,13 +234,13 @@ static double step_cost(const TaskDev &t) {
     return c;
 }
 
-// Paths per thread per tile: enough tiles to fill the GPU several times over,
-// few enough that per-tile reductions stay negligible.
+// Rounds per warp tile: enough tiles to keep every warp slot of the GPU busy
+// several times over, few enough that per-tile records stay negligible.
 int choose_ppt(int64_t n_paths, int64_t total_paths_all, int sm_count) {
-    const int64_t target_tiles = static_cast<int64_t>(sm_count) * 8 * 16;
-    int64_t ppt = total_paths_all / (target_tiles * kPathBlock);
-    ppt = std::max<int64_t>(1, std::min<int64_t>(ppt, 32));
-    const int64_t need = (n_paths + kPathBlock - 1) / kPathBlock;
+    const int64_t target_tiles = static_cast<int64_t>(sm_count) * 32 * 12;
+    int64_t ppt = total_paths_all / (target_tiles * kWarpTilePaths);
+    ppt = std::max<int64_t>(1, std::min<int64_t>(ppt, 64));
+    const int64_t need = (n_paths + kWarpTilePaths - 1) / kWarpTilePaths;
     ppt = std::min<int64_t>(ppt, std::max<int64_t>(1, need));
     return static_cast<int>(ppt);
 }
@@ -321,8 +325,11 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         }
     }
     if (!plain) {
+        // group by kernel (precision, model, scheme); longest tiles first inside a group
         std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
             if (a.t.precision != b.t.precision) return a.t.precision < b.t.precision;
+            if (a.t.model != b.t.model) return a.t.model < b.t.model;
+            if (a.t.scheme != b.t.scheme) return a.t.scheme < b.t.scheme;
             return a.cost > b.cost;
         });
     }
@@ -378,25 +385,27 @@ qk_status run_plan(qk_handle *h, Plan &plan) {
         if (plan.plain) {
             for (size_t i = 0; i < nt; ++i) {
                 const TaskDev &t = plan.tasks[i];
-                const int per_sm = price_tiles_max_blocks_per_sm(t.precision);
+                const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme);
                 const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
                 // one task: its own queue cursor, its own tile range (prefix of one task = itself)
-                QK_CUDA_TRY(launch_price_tiles(t.precision, grid, h->stream, dt + i, dp + i, 1, t.tile_begin,
-                                               t.tile_begin + t.n_tiles, dc + i, dpart));
+                QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
+                                               t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart));
                 h->launches++;
             }
         } else {
             size_t b = 0;
             while (b < nt) {
                 size_t e = b;
-                while (e < nt && plan.tasks[e].precision == plan.tasks[b].precision) ++e;
-                const int prec = plan.tasks[b].precision;
+                const TaskDev &tb = plan.tasks[b];
+                while (e < nt && plan.tasks[e].precision == tb.precision && plan.tasks[e].model == tb.model &&
+                       plan.tasks[e].scheme == tb.scheme)
+                    ++e;
                 const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
-                const int64_t slots = slots_end - plan.tasks[b].tile_begin;
-                const int per_sm = price_tiles_max_blocks_per_sm(prec);
+                const int64_t slots = slots_end - tb.tile_begin;
+                const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme);
                 const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
-                QK_CUDA_TRY(launch_price_tiles(prec, grid, h->stream, dt + b, dp + b, static_cast<int32_t>(e - b),
-                                               plan.tasks[b].tile_begin, slots_end, dc + b, dpart));
+                QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
+                                               static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart));
                 h->launches++;
                 b = e;
             }

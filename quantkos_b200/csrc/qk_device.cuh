@@ -29,10 +29,11 @@ struct U4 {
 __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t lo0 = kPhiloxM0 * c.x;
-        const uint32_t hi0 = __umulhi(kPhiloxM0, c.x);
-        const uint32_t lo1 = kPhiloxM1 * c.z;
-        const uint32_t hi1 = __umulhi(kPhiloxM1, c.z);
+        // one 32x32 -> 64-bit multiply per product (IMAD.WIDE.U32)
+        const uint64_t p0 = static_cast<uint64_t>(kPhiloxM0) * c.x;
+        const uint64_t p1 = static_cast<uint64_t>(kPhiloxM1) * c.z;
+        const uint32_t lo0 = static_cast<uint32_t>(p0), hi0 = static_cast<uint32_t>(p0 >> 32);
+        const uint32_t lo1 = static_cast<uint32_t>(p1), hi1 = static_cast<uint32_t>(p1 >> 32);
         c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
         k0 += kPhiloxW0;
         k1 += kPhiloxW1;
@@ -47,13 +48,39 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
 template <class R>
 struct Math;
 
+// Single SFU instructions (hand-written PTX): approximate base-2 exponential and
+// logarithm, reciprocal and square root, flushing subnormals to zero.
+__device__ __forceinline__ float ptx_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_lg2(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_sqrt(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <>
 struct Math<float> {
-    static __device__ __forceinline__ float exp(float x) { return __expf(x); }
-    static __device__ __forceinline__ float log(float x) { return __logf(x); }
-    // sqrt through one MUFU.RSQ; arguments here are >= 0 (variances, moment ratios)
-    static __device__ __forceinline__ float sqrt(float x) { return x > 1.0e-36f ? x * rsqrtf(x) : 0.0f; }
-    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static constexpr float kLog2e = 1.44269504088896341f;
+    static constexpr float kLn2 = 0.693147180559945309f;
+    static __device__ __forceinline__ float exp(float x) { return ptx_ex2(x * kLog2e); }
+    static __device__ __forceinline__ float log(float x) { return ptx_lg2(x) * kLn2; }
+    // arguments are >= 0 here (variances, moment ratios); sqrt.approx(0) = 0
+    static __device__ __forceinline__ float sqrt(float x) { return ptx_sqrt(x); }
+    static __device__ __forceinline__ float rcp(float x) { return ptx_rcp(x); }
+    static __device__ __forceinline__ float div(float a, float b) { return a * ptx_rcp(b); }
     static __device__ __forceinline__ float erf(float x) { return erff(x); }
     // uniform in (0,1): (k + 1/2) / 2^23, k = top 23 bits of the word
     static __device__ __forceinline__ float u01(uint32_t w) {
@@ -63,7 +90,7 @@ struct Math<float> {
     static __device__ __forceinline__ void box_muller(uint32_t w1, uint32_t w2, float &z1, float &z2) {
         const float u1 = u01(w1);
         const float u2 = u01(w2);
-        const float rad = sqrt(-2.0f * log(u1));
+        const float rad = ptx_sqrt(-2.0f * kLn2 * ptx_lg2(u1));
         float s, c;
         __sincosf(6.28318530717958648f * (u2 - 0.5f), &s, &c);
         z1 = rad * c;
@@ -76,6 +103,7 @@ struct Math<double> {
     static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
     static __device__ __forceinline__ double log(double x) { return ::log(x); }
     static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
     static __device__ __forceinline__ double erf(double x) { return ::erf(x); }
     static __device__ __forceinline__ double u01(uint32_t w) {
@@ -101,41 +129,40 @@ __device__ __forceinline__ R rmin(R a, R b) { return fmin(a, b); }
 // Draw sources.  A step asks for: one normal pair (Z1, Z2); Bates steps then ask
 // for Poisson uniforms one at a time and, when a jump occurred, one jump normal.
 //
-// Philox layout per path p of stream s:
-//   Heston: block floor(n/2), domain 0; words (x,y) feed step 2k, (z,w) step 2k+1.
-//   Bates:  block n, domain 0: (x,y) -> normal pair, z -> 1st Poisson uniform,
-//           w -> 2nd Poisson uniform; block n, domain 1: (x,y) -> jump normal,
-//           (z,w) -> Poisson uniforms 3,4; block n, domain d>=2: uniforms 4d-3 .. 4d.
+// Philox layout per path p of stream s (counter = (block, p, s, domain)):
+//   normal pair of step n:        domain 0, block floor(n/2), words (x,y) if n even, (z,w) if odd;
+//   1st Poisson uniform of step n: domain 2, block floor(n/4), word n mod 4;
+//   jump normal of step n:         domain 1, block n, Box-Muller of words (x,y), first output;
+//   Poisson uniforms 2, 3:         domain 1, block n, words z, w;
+//   Poisson uniform k >= 4:        domain 3 + (k-4)/4, block n, word (k-4) mod 4.
+// A step costs half a Philox block for the normals and, under Bates, a quarter
+// block for the jump test; the rest is drawn only on the rare steps with a jump.
 // ============================================================================
 template <class R>
-struct PhiloxBatesStep {
-    uint32_t k0, k1, path, stream;
-    int step;
-    U4 w0;      // domain-0 words of this step
-    U4 wx;      // current extra-domain block
-    int used;   // Poisson uniforms consumed in this step
-    int domain; // extra domain currently held in wx (0 = none)
+struct PhiloxJumpDraws {
+    uint32_t k0, k1, path, stream, step;
+    R first;    // the step's first Poisson uniform
+    int used;   // Poisson uniforms consumed so far in this step
+    int domain; // block currently held in wx (0 = none)
+    U4 wx;
 
-    __device__ __forceinline__ void normal_pair(R &z1, R &z2) { Math<R>::box_muller(w0.x, w0.y, z1, z2); }
-    __device__ __forceinline__ U4 extra(int d) {
-        return philox4x32_10(U4{static_cast<uint32_t>(step), path, stream, static_cast<uint32_t>(d)}, k0, k1);
+    __device__ __forceinline__ U4 block(uint32_t d) {
+        return philox4x32_10(U4{step, path, stream, d}, k0, k1);
     }
     __device__ __forceinline__ R uniform() {
         const int k = used++;
-        if (k == 0) return Math<R>::u01(w0.z);
-        if (k == 1) return Math<R>::u01(w0.w);
-        // uniform k (0-based) >= 2: domain 1 words z,w for k = 2,3; domain 2 + (k-4)/4 words x..w after
-        const int d = (k < 4) ? 1 : 2 + (k - 4) / 4;
+        if (k == 0) return first;
+        const int d = (k < 3) ? 1 : 3 + (k - 3) / 4;
         if (domain != d) {
-            wx = extra(d);
+            wx = block(static_cast<uint32_t>(d));
             domain = d;
         }
-        const int slot = (k < 4) ? k : ((k - 4) & 3);
+        const int slot = (k < 3) ? k + 1 : ((k - 3) & 3);
         const uint32_t word = slot == 0 ? wx.x : (slot == 1 ? wx.y : (slot == 2 ? wx.z : wx.w));
         return Math<R>::u01(word);
     }
     __device__ __forceinline__ R jump_normal() {
-        const U4 j = extra(1);
+        const U4 j = block(1u);
         R z1, z2;
         Math<R>::box_muller(j.x, j.y, z1, z2);
         return z1;
@@ -209,7 +236,7 @@ __device__ __forceinline__ void step_qe(const StepConst<R> &p, R &S, R &v, R Zv,
         vn = R(0);
         logM = R(0);
     } else {
-        const R inv_m = Math<R>::div(R(1), m);
+        const R inv_m = Math<R>::rcp(m);
         const R psi = s2 * inv_m * inv_m;
         if (psi <= p.eps) {
             vn = m;
@@ -260,20 +287,23 @@ __device__ __forceinline__ void heston_step(const StepConst<R> &p, R &S, R &v, R
 
 // Bates jump part after the (drift-compensated) Heston step: MSchemes.hpp:493-526.
 // Knuth's Poisson draw: multiply uniforms until the product drops below exp(-lambda dt).
+// `prod` holds the first uniform, already known to be >= exp(-lambda dt) (a jump).
+template <class R, class Draws>
+__device__ __noinline__ R jump_factor(const StepConst<R> &p, R prod, Draws &d) {
+    int N = 0;
+    do {
+        ++N;
+        prod *= d.uniform();
+    } while (prod >= p.exp_m_lambda_dt && N < kMaxJumpsPerStep);
+    const R Z = d.jump_normal();
+    const R rN = static_cast<R>(N);
+    return Math<R>::exp(rN * p.mu_j + Math<R>::sqrt(rN) * p.sigma_j * Z);
+}
+
 template <class R, class Draws>
 __device__ __forceinline__ void bates_jump(const StepConst<R> &p, R &S, Draws &d) {
-    R prod = d.uniform();
-    if (prod >= p.exp_m_lambda_dt) {
-        int N = 0;
-        do {
-            ++N;
-            prod *= d.uniform();
-        } while (prod >= p.exp_m_lambda_dt && N < kMaxJumpsPerStep);
-        const R Z = d.jump_normal();
-        const R rN = static_cast<R>(N);
-        const R mag = Math<R>::exp(rN * p.mu_j + Math<R>::sqrt(rN) * p.sigma_j * Z);
-        S *= mag;
-    }
+    const R first = d.uniform();
+    if (first >= p.exp_m_lambda_dt) S *= jump_factor<R>(p, first, d);
 }
 
 template <class R, int MODEL, int SCHEME, class Draws>

@@ -66,6 +66,7 @@ struct TaskDev {
     int32_t precision;     // qk_precision
     uint32_t key0, key1;   // Philox key = seed
     uint32_t stream;       // Philox counter word 2 (common random numbers across bumps)
+    uint32_t jump_kmin;    // FP32 jump test: a step jumps iff (first Poisson word >> 9) >= jump_kmin
     int64_t n_paths;
     int64_t tile_begin;    // first queue slot of the task (tiles of a task are consecutive)
     int64_t partial_base;  // first per-tile moments record of the task

@@ -7,11 +7,16 @@
 
 namespace qk {
 
-constexpr int kPathBlock = 256;  // threads (= paths) per pricing tile
+constexpr int kPathBlock = 256;     // threads per block of the path kernels
+constexpr int kWarpTilePaths = 32;  // paths per round of a warp tile (one per lane)
+#ifndef QK_PATH_MIN_BLOCKS_FP32
+#define QK_PATH_MIN_BLOCKS_FP32 4
+#endif
+constexpr int kPathMinBlocksFp32 = QK_PATH_MIN_BLOCKS_FP32;  // resident blocks per SM the FP32 path kernel is register-budgeted for
 
-cudaError_t launch_price_tiles(int precision, int grid, cudaStream_t s, const TaskDev *tasks, const int64_t *prefix,
-                               int32_t n_tasks, int64_t slot_begin, int64_t slot_end, unsigned long long *cursor,
-                               Moments *partials);
+cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
+                               const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
+                               unsigned long long *cursor, Moments *partials);
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
                                TaskMoments *out);
 cudaError_t launch_slab_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t first_path, int64_t count,
@@ -19,7 +24,7 @@ cudaError_t launch_slab_paths(int precision, cudaStream_t s, const TaskDev *task
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
                               int umax, int n, double *S_out, double *v_out, int *status);
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);
-int price_tiles_max_blocks_per_sm(int precision);
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme);
 // Times a kernel of independent ex2.approx chains; returns its duration and MUFU op count.
 cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
                              double *ops);

@@ -18,7 +18,7 @@ namespace qk {
 template <class R>
 struct PathState {
     R S, v;
-    double ssum;
+    double ssum;  // running sum of S for the Asian average, in double (Payoff.hpp:87, 110)
     R smax, smin;
 };
 
@@ -44,59 +44,81 @@ struct SlabSink {
     }
 };
 
+// Steps are taken in chunks of kSumChunk; the Asian running sum is accumulated in
+// the working precision inside a chunk and folded into the FP64 sum after it.
+constexpr int kSumChunk = 16;
+
 template <class R>
-__device__ __forceinline__ void track(PathState<R> &st) {
-    st.ssum += static_cast<double>(st.S);
+__device__ __forceinline__ void track(PathState<R> &st, R &blk) {
+    blk += st.S;
     st.smax = rmax(st.smax, st.S);
     st.smin = rmin(st.smin, st.S);
 }
 
+// The step's first Poisson uniform decides whether a jump happened (Knuth's loop
+// continues only if it is >= exp(-lambda dt)).  FP32 compares the word directly:
+// (w >> 9) >= kmin  <=>  u01(w) >= exp(-lambda dt) in float, kmin precomputed exactly.
+template <class R>
+__device__ __forceinline__ bool jump_test(uint32_t word, const StepConst<R> &p, uint32_t kmin) {
+    if constexpr (sizeof(R) == 4) {
+        return (word >> 9) >= kmin;
+    } else {
+        return Math<R>::u01(word) >= p.exp_m_lambda_dt;
+    }
+}
+
+template <class R, int MODEL, int SCHEME>
+__device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st, uint32_t wa, uint32_t wb,
+                                         uint32_t wpois, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path,
+                                         uint32_t stream, int n) {
+    R z1, z2;
+    Math<R>::box_muller(wa, wb, z1, z2);
+    heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
+    if constexpr (MODEL == kBates) {
+        if (jump_test<R>(wpois, p, kmin)) {
+            PhiloxJumpDraws<R> d{k0, k1, path, stream, static_cast<uint32_t>(n), Math<R>::u01(wpois), 1, 0, U4{0, 0, 0, 0}};
+            st.S *= jump_factor<R>(p, d.first, d);
+        }
+    }
+}
+
 template <class R, int MODEL, int SCHEME, class Sink>
 __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0, int n_steps, uint32_t k0,
-                                              uint32_t k1, uint32_t path, uint32_t stream, PathState<R> &st,
-                                              const Sink &sink) {
+                                              uint32_t k1, uint32_t path, uint32_t stream, uint32_t kmin,
+                                              PathState<R> &st, const Sink &sink) {
     st.S = S0;
     st.v = v0;
     st.ssum = 0.0;
     st.smax = S0;
     st.smin = S0;
-    if constexpr (MODEL == kHeston) {
-        int n = 0;
-        for (; n + 1 < n_steps; n += 2) {
+    for (int n0 = 0; n0 < n_steps; n0 += kSumChunk) {
+        const int n1 = min(n0 + kSumChunk, n_steps);
+        R blk = R(0);
+        U4 wp{0u, 0u, 0u, 0u};  // Poisson words of steps 4m .. 4m+3 (n0 is a multiple of 4)
+        int n = n0;
+        for (; n + 1 < n1; n += 2) {
             const U4 w = philox4x32_10(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u}, k0, k1);
-            R z1, z2;
-            Math<R>::box_muller(w.x, w.y, z1, z2);
-            heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
-            track(st);
+            if constexpr (MODEL == kBates) {
+                if ((n & 3) == 0) wp = philox4x32_10(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u}, k0, k1);
+            }
+            const bool lo = (n & 3) == 0;
+            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, lo ? wp.x : wp.z, kmin, k0, k1, path, stream, n);
+            track(st, blk);
             sink(n, st.S, st.v);
-            Math<R>::box_muller(w.z, w.w, z1, z2);
-            heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
-            track(st);
+            one_step<R, MODEL, SCHEME>(p, st, w.z, w.w, lo ? wp.y : wp.w, kmin, k0, k1, path, stream, n + 1);
+            track(st, blk);
             sink(n + 1, st.S, st.v);
         }
-        if (n < n_steps) {
+        if (n < n1) {
             const U4 w = philox4x32_10(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u}, k0, k1);
-            R z1, z2;
-            Math<R>::box_muller(w.x, w.y, z1, z2);
-            heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
-            track(st);
+            if constexpr (MODEL == kBates) {
+                if ((n & 3) == 0) wp = philox4x32_10(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u}, k0, k1);
+            }
+            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, (n & 3) == 0 ? wp.x : wp.z, kmin, k0, k1, path, stream, n);
+            track(st, blk);
             sink(n, st.S, st.v);
         }
-    } else {
-        for (int n = 0; n < n_steps; ++n) {
-            PhiloxBatesStep<R> d;
-            d.k0 = k0;
-            d.k1 = k1;
-            d.path = path;
-            d.stream = stream;
-            d.step = n;
-            d.w0 = philox4x32_10(U4{static_cast<uint32_t>(n), path, stream, 0u}, k0, k1);
-            d.used = 0;
-            d.domain = 0;
-            evolve_step<R, kBates, SCHEME>(p, st.S, st.v, d);
-            track(st);
-            sink(n, st.S, st.v);
-        }
+        st.ssum += static_cast<double>(blk);
     }
 }
 
@@ -112,13 +134,14 @@ __device__ __forceinline__ void simulate_dispatch(const TaskDev &t, const StepCo
                                                   PathState<R> &st, const Sink &sink) {
     const R S0 = static_cast<R>(t.S0);
     const R v0 = static_cast<R>(t.v0);
+    const uint32_t km = t.jump_kmin;
     switch (t.model * 3 + t.scheme) {
-        case 0: simulate_path<R, kHeston, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
-        case 1: simulate_path<R, kHeston, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
-        case 2: simulate_path<R, kHeston, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
-        case 3: simulate_path<R, kBates, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
-        case 4: simulate_path<R, kBates, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
-        default: simulate_path<R, kBates, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, st, sink); break;
+        case 0: simulate_path<R, kHeston, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 1: simulate_path<R, kHeston, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 2: simulate_path<R, kHeston, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 3: simulate_path<R, kBates, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 4: simulate_path<R, kBates, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        default: simulate_path<R, kBates, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
     }
 }
 
@@ -141,69 +164,80 @@ __device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int
     return lo;
 }
 
-template <class R>
-__global__ void __launch_bounds__(kPathBlock) price_tiles_kernel(const TaskDev *__restrict__ tasks,
-                                                                const int64_t *__restrict__ prefix, int32_t n_tasks,
-                                                                int64_t slot_begin, int64_t slot_end,
-                                                                unsigned long long *__restrict__ cursor,
-                                                                Moments *__restrict__ partials) {
-    __shared__ int64_t s_slot;
-    __shared__ Moments s_warp[QK_MAX_PAYOFFS][kPathBlock / 32];
+template <class R, int MODEL, int SCHEME>
+__global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp32 : 1)
+    price_tiles_kernel(const TaskDev *__restrict__ tasks, const int64_t *__restrict__ prefix, int32_t n_tasks,
+                       int64_t slot_begin, int64_t slot_end, unsigned long long *__restrict__ cursor,
+                       Moments *__restrict__ partials) {
+    // Every warp is an independent worker: it pops a tile (kWarpTilePaths * ppt paths of one
+    // task), keeps the tile's running moments per leg in its own shared-memory slots and
+    // writes one record per leg.  No block-wide barrier anywhere.
+    __shared__ Moments s_acc[kPathBlock / 32][QK_MAX_PAYOFFS];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);  // OptionPricer.hpp:316
+    Moments *acc = s_acc[warp];
 
     for (;;) {
-        if (threadIdx.x == 0) {
-            const int64_t q = slot_begin + static_cast<int64_t>(atomicAdd(cursor, 1ull));
-            s_slot = q < slot_end ? q : -1;
-        }
-        __syncthreads();
-        const int64_t slot = s_slot;
-        __syncthreads();
-        if (slot < 0) return;
+        long long q = 0;
+        if (lane == 0) q = slot_begin + static_cast<long long>(atomicAdd(cursor, 1ull));
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= slot_end) return;
 
-        const int ti = find_task(prefix, n_tasks, slot);
+        const int ti = find_task(prefix, n_tasks, q);
         const TaskDev &t = tasks[ti];
-        const int64_t tile = slot - t.tile_begin;
+        const int64_t tile = q - t.tile_begin;
         const StepConst<R> p = task_const<R>(t);
         const int np = t.n_payoffs;
         const int ppt = t.ppt;
-        const int64_t tile_first = tile * static_cast<int64_t>(kPathBlock) * ppt;
-        // lane 0 of each warp keeps the warp's running moments in shared memory
-        if (lane == 0)
-            for (int k = 0; k < np; ++k) s_warp[k][warp] = Moments{0.0, 0.0, 0.0, 0.0};
+        const int n_steps = t.n_steps;
+        const int64_t n_paths = t.n_paths;
+        const uint32_t k0 = t.key0, k1 = t.key1, stream = t.stream, kmin = t.jump_kmin;
+        const R S0 = static_cast<R>(t.S0), v0 = static_cast<R>(t.v0);
+        const int64_t tile_first = tile * static_cast<int64_t>(kWarpTilePaths) * ppt;
+        if (lane < np) acc[lane] = Moments{0.0, 0.0, 0.0, 0.0};
+        __syncwarp();
 
-        for (int j = 0; j < ppt; ++j) {
-            const int64_t path = tile_first + static_cast<int64_t>(j) * kPathBlock + threadIdx.x;
-            const bool active = path < t.n_paths;
-            if (__syncthreads_or(active) == 0) break;
+        const int64_t left = n_paths - tile_first;
+        const int rounds =
+            static_cast<int>(min(static_cast<int64_t>(ppt), (left + kWarpTilePaths - 1) / kWarpTilePaths));
+        for (int j = 0; j < rounds; ++j) {
+            const int64_t path = tile_first + static_cast<int64_t>(j) * kWarpTilePaths + lane;
+            const bool active = path < n_paths;
             PathState<R> st;
             if (active) {
-                simulate_dispatch<R>(t, p, static_cast<uint32_t>(path), st, NoSink{});
+                simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, k0, k1, static_cast<uint32_t>(path), stream, kmin,
+                                                st, NoSink{});
             } else {
                 st.S = st.smax = st.smin = R(0);
                 st.ssum = 0.0;
             }
             for (int k = 0; k < np; ++k) {
                 const PayoffSpec ps = t.pay[k];
-                const R x = active ? final_payoff<R>(ps, st.S, st.ssum, st.smax, st.smin, t.n_steps) : R(0);
+                const R x = active ? final_payoff<R>(ps, st.S, st.ssum, st.smax, st.smin, n_steps) : R(0);
                 const Moments wm = warp_moments(static_cast<double>(x), active, x > eps_payoff);
-                if (lane == 0) s_warp[k][warp] = chan_merge(s_warp[k][warp], wm);
+                if (lane == 0) acc[k] = chan_merge(acc[k], wm);
             }
         }
-        __syncthreads();
-        if (warp == 0) {
-            for (int k = 0; k < np; ++k) {
-                Moments m = lane < kPathBlock / 32 ? s_warp[k][lane] : Moments{0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const Moments o = shfl_down_moments(m, off);
-                    m = chan_merge(m, o);
-                }
-                if (lane == 0) partials[t.partial_base + tile * np + k] = m;
-            }
-        }
+        __syncwarp();
+        if (lane < np) partials[t.partial_base + tile * np + lane] = acc[lane];
+        __syncwarp();
+    }
+}
+
+template <class R>
+using PriceKernel = void (*)(const TaskDev *, const int64_t *, int32_t, int64_t, int64_t, unsigned long long *,
+                             Moments *);
+
+template <class R>
+__host__ PriceKernel<R> price_kernel_for(int model, int scheme) {
+    switch (model * 3 + scheme) {
+        case 0: return price_tiles_kernel<R, kHeston, kEuler>;
+        case 1: return price_tiles_kernel<R, kHeston, kMilstein>;
+        case 2: return price_tiles_kernel<R, kHeston, kQE>;
+        case 3: return price_tiles_kernel<R, kBates, kEuler>;
+        case 4: return price_tiles_kernel<R, kBates, kMilstein>;
+        default: return price_tiles_kernel<R, kBates, kQE>;
     }
 }
 
@@ -294,13 +328,15 @@ __global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double
 // ----------------------------------------------------------------------------
 // Launchers
 // ----------------------------------------------------------------------------
-cudaError_t launch_price_tiles(int precision, int grid, cudaStream_t s, const TaskDev *tasks, const int64_t *prefix,
-                               int32_t n_tasks, int64_t slot_begin, int64_t slot_end, unsigned long long *cursor,
-                               Moments *partials) {
+cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
+                               const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
+                               unsigned long long *cursor, Moments *partials) {
     if (precision == QK_FP32)
-        price_tiles_kernel<float><<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials);
+        price_kernel_for<float>(model, scheme)<<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin,
+                                                                           slot_end, cursor, partials);
     else
-        price_tiles_kernel<double><<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials);
+        price_kernel_for<double>(model, scheme)<<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin,
+                                                                            slot_end, cursor, partials);
     return cudaGetLastError();
 }
 
@@ -370,12 +406,12 @@ cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEven
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
-int price_tiles_max_blocks_per_sm(int precision) {
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme) {
     int nb = 0;
     if (precision == QK_FP32)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_tiles_kernel<float>, kPathBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<float>(model, scheme), kPathBlock, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_tiles_kernel<double>, kPathBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<double>(model, scheme), kPathBlock, 0);
     return nb > 0 ? nb : 1;
 }
 

@@ -56,7 +56,7 @@ size_t footprint(const qk_contract &c, const qk_greeks &g) {
         const size_t slabs = c.lsm_basis == QK_LSM_POLY_SV ? 2 : 1;
         bytes += D * ld * esz * slabs + ld * esz;  // slabs are reused across the bumps of one request
     } else {
-        const size_t tiles = (static_cast<size_t>(c.n_paths) + qk::kPathBlock - 1) / qk::kPathBlock;
+        const size_t tiles = (static_cast<size_t>(c.n_paths) + qk::kWarpTilePaths - 1) / qk::kWarpTilePaths;
         bytes += roles * tiles * c.n_payoffs * sizeof(qk::Moments);
     }
     return bytes;
