@@ -185,6 +185,20 @@ qk_status qk_batch_prepare(qk_handle *h, const qk_contract *c, int32_t n, const 
 qk_status qk_batch_run(qk_handle *h);
 qk_status qk_batch_fetch(qk_handle *h, qk_result *out, int32_t n);
 
+/* qk_price_noalloc — no counterpart in the reference.  The base price (no Greeks)
+ * of one forward contract for callers that cannot allocate device memory on the
+ * pricing path (a host application owning all GPU memory through its own pool,
+ * or a latency-critical caller that cannot take cudaMalloc/cudaFree and their
+ * device synchronisation between requests).  Same kernels as qk_price_batch; all
+ * scratch lives in one fixed device array of about 4.1 MiB reserved per device
+ * when the library loads; nothing is allocated and no handle is needed.
+ * Limit: ceil(n_paths / 2048) * n_payoffs <= 131072 (QK_ERR_CAPACITY beyond).
+ * The first call on a device looks up the array's address with that device
+ * current: make it before any stream capture.  Calls share the array: calls
+ * whose GPU work overlaps race, so serialize them.  `stream` is a cudaStream_t
+ * (NULL = default stream); the call returns after its work has finished. */
+qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_result *out);
+
 /* ---------------------------------------------------------------- parity harness
  * qk_step_trace — SDEScheme<M,S>::evolve_step with fed draws
  * (include/core/schemes/markovian/MSchemes.hpp:133-156, 229-253, 363-442, 493-526),

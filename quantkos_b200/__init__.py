@@ -12,7 +12,7 @@ from ._lib import (ANDERSEN_QE, AMERICAN, ASIAN, BARRIER_DOWN_IN, BARRIER_DOWN_O
                    IMPLICIT_MILSTEIN, LOOKBACK_FIXED, LOOKBACK_FLOATING, LSM_LAGUERRE3, LSM_POLY_SV, PUT)
 from .engine import (Handle, MCDispatcher, MCGreeks, MCOpPrices, MCResults, Parser, PreparedBatch,  # noqa: F401
                      QuantKosError, QuantKosInvalidArgument, Server, UInputs, default_handle, make_contract,
-                     make_greeks, n_steps_for, paths, payoff, price_batch, price_plain, step_trace)
+                     make_greeks, n_steps_for, paths, payoff, price_batch, price_noalloc, price_plain, step_trace)
 
 
 def load_native():

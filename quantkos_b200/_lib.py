@@ -123,6 +123,7 @@ SIGNATURES = {
     "qk_batch_prepare": (C.c_int, [_VP, _P(Contract), C.c_int32, _P(Greeks)]),
     "qk_batch_run": (C.c_int, [_VP]),
     "qk_batch_fetch": (C.c_int, [_VP, _P(Result), C.c_int32]),
+    "qk_price_noalloc": (C.c_int, [_P(Contract), _VP, _P(Result)]),
     "qk_step_trace": (C.c_int, [C.c_int32, _P(Contract), _P(C.c_double), _P(C.c_double), C.c_int32, C.c_int32,
                                 _P(C.c_double), _P(C.c_double)]),
     "qk_paths_dump": (C.c_int, [_VP, _P(Contract), C.c_int64, C.c_int64, _P(C.c_double), _P(C.c_double)]),

@@ -168,6 +168,16 @@ def price_batch(contracts: Sequence[L.Contract], greeks: L.Greeks | None = None,
     return [result_to_dict(out[i]) for i in range(n)]
 
 
+def price_noalloc(contract: L.Contract, stream: int = 0) -> dict:
+    """Base price of one forward contract without any device allocation (fixed scratch).
+
+    For callers that may not allocate GPU memory while pricing; see qk_price_noalloc in
+    include/quantkos_b200.h for the size limit and the rules of use."""
+    out = L.Result()
+    check(L.lib().qk_price_noalloc(C.byref(contract), C.c_void_p(stream or None), C.byref(out)), "qk_price_noalloc")
+    return result_to_dict(out)
+
+
 class PreparedBatch:
     """Device-resident task set: prepare once, run many times (inputs stay in HBM)."""
 
