@@ -56,6 +56,10 @@ def parse_args():
     ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--paths", type=int, default=N_PATHS,
                     help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
+    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve"], default="bates5",
+                    help="bates5 (default): the headline line; the others measure the remaining workloads")
+    ap.add_argument("--subset", type=int, default=128, help="batch: contracts priced by both engines")
+    ap.add_argument("--requests", type=int, default=20_000, help="serve: number of requests")
     return ap.parse_args()
 
 
@@ -173,10 +177,162 @@ def run_reference_arm(args) -> None:
 
 
 # ----------------------------------------------------------------------------- our arm
+# ----------------------------------------------------------------------------- other workloads
+def _timed(torch, ext, fn, steps: int, flush=None) -> list[float]:
+    """Device-time (CUDA events on the engine stream) of `steps` calls of fn, L2 flushed between."""
+    out = []
+    for i in range(steps):
+        if flush is not None:
+            flush.fill_(float(i))
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        fn()
+        b.record(ext)
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def run_other_workload(args) -> None:
+    import torch
+
+    import quantkos_b200 as qk
+    from quantkos_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    h = qk.Handle(0)
+    ext = torch.cuda.ExternalStream(h.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    line: dict = {"metric": METRIC, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                  "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic"}
+    sampler = ClockSampler(0)
+    if args.workload == "plain":
+        c = W.plain_heston_euler()
+        for _ in range(args.warmup):
+            qk.price_plain(c, None, h)
+        launches = 0
+        with sampler:
+            ts = _timed(torch, ext, lambda: qk.price_plain(c, None, h), args.steps, flush)
+        r = qk.price_plain(c, None, h)["legs"][0]
+        ps = c.n_paths * c.n_steps
+        line.update(value=ps / (statistics.mean(ts) * 1e-3), ms_per_step=statistics.mean(ts), dtype="f64",
+                    config={"workload": "heston_euler_european_call_1048576x252_fp64_plain", "price": r["price"],
+                            "std_error": r["std_error"]},
+                    gpu_launches=args.steps * h.last_timing()["launches"])
+    elif args.workload == "lsm":
+        c32 = W.american_lsm(precision=qk.FP32)
+        c64 = W.american_lsm(precision=qk.FP64)
+        for _ in range(args.warmup):
+            qk.price_batch([c32], None, h)
+        with sampler:
+            ts = _timed(torch, ext, lambda: qk.price_batch([c32], None, h), args.steps, flush)
+        t = h.last_timing()
+        r32 = qk.price_batch([c32], None, h)[0]["legs"][0]
+        qk.price_plain(c64, None, h)
+        t64 = _timed(torch, ext, lambda: qk.price_plain(c64, None, h), 1, flush)[0]
+        r64 = qk.price_plain(c64, None, h)["legs"][0]
+        ps = c32.n_paths * c32.n_steps
+        # backward sweep: algorithmic 16 B per path per date (S, v slab read + cash flow read/write, FP32)
+        sweep_bytes = 16.0 * c32.n_paths * 50
+        ms = statistics.mean(ts)
+        line.update(value=ps / (ms * 1e-3), ms_per_step=ms, dtype="f32",
+                    config={"workload": "american_put_lsm_heston_qe_4194304x250_50dates_polysv", "price": r32["price"],
+                            "std_error": r32["std_error"], "price_fp64": r64["price"], "std_error_fp64": r64["std_error"],
+                            "fp64_plain_ms": t64, "speedup_vs_fp64_plain": t64 / ms},
+                    roofline={"bound": "hbm", "achieved": sweep_bytes / (t["reduce_ms"] * 1e-3) / 1e9,
+                              "peak": json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs")
+                              if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0,
+                              "unit": "GB/s", "kernel": "LSM backward sweep (all dates)",
+                              "sweep_ms": t["reduce_ms"], "forward_ms": t["device_ms"] - t["reduce_ms"]},
+                    gpu_launches=args.steps * t["launches"])
+        line["roofline"]["frac"] = line["roofline"]["achieved"] / line["roofline"]["peak"]
+    elif args.workload == "batch":
+        g = W.batch_greeks()
+        full = W.mixed_batch()
+        sub = full[:args.subset]
+        sub64 = W.mixed_batch(args.subset, precision=qk.FP64)
+        qk.price_batch(sub, g, h)
+        t_sub = _timed(torch, ext, lambda: qk.price_batch(sub, g, h), 1, flush)[0]
+        res32 = qk.price_batch(sub, g, h)
+        qk.price_plain(sub64[0], g, h)
+        res64 = []
+
+        def plain_all():
+            res64.clear()
+            for c in sub64:
+                res64.append(qk.price_plain(c, g, h))
+
+        t_plain = _timed(torch, ext, plain_all, 1, flush)[0]
+        with sampler:
+            t_full = _timed(torch, ext, lambda: qk.price_batch(full, g, h), max(1, args.steps // 10), flush)
+        tf = h.last_timing()
+        ms = statistics.mean(t_full)
+        se_ratio = statistics.mean(a["legs"][0]["std_error"] / b["legs"][0]["std_error"]
+                                   for a, b in zip(res32, res64) if b["legs"][0]["std_error"] > 0)
+        within = sum(abs(a["legs"][0]["price"] - b["legs"][0]["price"]) <= 3.0 * b["legs"][0]["std_error"] + 1e-12
+                     for a, b in zip(res32, res64)) / len(sub)
+        line.update(metric="contracts/s", unit="contracts/s", value=len(full) / (ms * 1e-3), ms_per_step=ms,
+                    dtype="f32",
+                    config={"workload": "mixed_4096_contracts_all_greeks_seed123",
+                            "path_steps": W.path_steps(full, g), "path_steps_per_s": W.path_steps(full, g) / (ms * 1e-3),
+                            "subset": len(sub), "subset_batched_contracts_per_s": len(sub) / (t_sub * 1e-3),
+                            "subset_plain_fp64_contracts_per_s": len(sub) / (t_plain * 1e-3),
+                            "speedup_vs_plain_fp64_same_subset": t_plain / t_sub,
+                            "mean_se_ratio_batched_over_plain": se_ratio,
+                            "subset_prices_within_3se_of_fp64": within},
+                    gpu_launches=tf["launches"])
+    else:  # serve
+        arrivals, contracts = W.serving_stream(args.requests)
+        srv = qk.Server(h, 0, 512)
+        # warm both lanes
+        for c in contracts[:8]:
+            srv.poll(srv.submit(c), 600_000)
+        srv.stop()
+        srv = qk.Server(h, 0, 512)
+        import threading
+        tickets = []
+        t0 = time.perf_counter()
+
+        def producer():
+            for t_arr, c in zip(arrivals, contracts):
+                now = time.perf_counter() - t0
+                if t_arr > now:
+                    time.sleep(t_arr - now)
+                tickets.append(srv.submit(c))
+
+        with sampler:
+            th = threading.Thread(target=producer)
+            th.start()
+            th.join()
+            for tk in tickets:
+                while srv.poll(tk, 1000) is None:
+                    pass
+        st = srv.stats()
+        srv.stop()
+        offered = W.path_steps(contracts)
+        line.update(metric="contracts/s", unit="contracts/s", value=st["contracts_per_s"], dtype="f32",
+                    ms_per_step=None,
+                    config={"workload": f"serving_{args.requests}_requests_poisson_2000_per_s_30pct_american",
+                            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"],
+                            "max_ms": st["max_ms"], "path_steps_per_s": st["path_steps_per_s"],
+                            "offered_path_steps": offered, "offered_path_steps_per_s": offered / arrivals[-1],
+                            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"]},
+                    gpu_launches=None)
+    pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    line["clocks"] = sampler.summary(pk.get("sm_max_mhz", 1965.0))
+    print(json.dumps(line), flush=True)
+    h.close()
+
+
 def main() -> None:
     args = parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload != "bates5":
+        run_other_workload(args)
         return
 
     import torch

@@ -1,0 +1,210 @@
+"""GPU: the system around the kernels — config-driven runs (MCDispatcher, .paths
+files, payoff percentiles, the CLI), the continuous-batching server, and the
+mixed batched workload against closed forms."""
+import math
+import os
+import struct
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from tests.helpers import load
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parent.parent
+
+YAML = """
+Market:
+  Price: 100.0
+  Variance: 0.04
+  r: 0.05
+  q: 0.02
+Options:
+  OptionType: {otype}
+  OptionRight: {right}
+  StrikePrice: 100.
+  BarrierPrice: 120.
+Model:
+  Heston:
+    k: 2.0
+    theta: 0.04
+    sigma: 0.3
+    rho: -0.7
+Numerics:
+  Scheme: AndersonQE
+Time:
+  T_End: 1.0
+  Inp_DT: 0.0078125
+MC:
+  Normalize_prices: true
+  N_Paths: 20000
+  RNG_Seed: 12345
+  analyze_risk_neutral_payoff_distribution: {dist}
+  compute_delta_et_gamma: {greeks}
+  Precision: {prec}
+  Engine: {engine}
+Output:
+  out_dir: "{out_dir}"
+  Name_Paths_Out_File: "{paths}"
+  Format: BIN
+"""
+
+
+def _cfg(qk, tmp_path, otype="European", right="Call", dist="false", greeks="false", prec="FP64", engine="plain",
+         paths=""):
+    return qk.Parser.parse_string(YAML.format(otype=otype, right=right, dist=dist, greeks=greeks, prec=prec,
+                                              engine=engine, out_dir=str(tmp_path), paths=paths))
+
+
+def test_dispatcher_matches_contract_path(qk, handle, oracle, tmp_path):
+    cfg = _cfg(qk, tmp_path, greeks="true")
+    res = qk.MCDispatcher(cfg, handle).launch_montecarlo()
+    k, g = cfg.to_contract()
+    o = oracle.price(k, g)["legs"][0]
+    assert res.OptionPrice.option_price == pytest.approx(o["price"], rel=1e-9)
+    assert res.Greeks.delta == pytest.approx(o["delta"], rel=1e-6)
+    assert res.Greeks.gamma == pytest.approx(o["gamma"], rel=1e-5, abs=1e-9)
+
+
+def test_paths_file_roundtrip(qk, handle, oracle, tmp_path):
+    """BinWriter / BinReader (include/IO/IOBinary.hpp:72-378): 40-byte header, row-major payload of
+    normalised prices; reading column j at t = (j+1) dt returns scaled prices (BinaryFormatTest)."""
+    cfg = _cfg(qk, tmp_path, paths="run.paths")
+    cfg.n_paths = 300
+    qk.MCDispatcher(cfg, handle).launch_montecarlo()
+    f = tmp_path / "run.paths"
+    data = f.read_bytes()
+    key, version, prec, n, steps = struct.unpack_from("<8siiii", data, 0)
+    dt, scale = struct.unpack_from("<dd", data, 24)
+    assert key == b"QUANTKOS" and version == 1 and prec == 8 and n == 300 and steps == 128
+    assert dt == pytest.approx(1.0 / 128) and scale == 100.0
+    payload = np.frombuffer(data, dtype=np.float64, offset=40).reshape(n, steps)
+    k, _ = cfg.to_contract()
+    S, _ = oracle.paths(k, 0, 300)
+    np.testing.assert_allclose(payload * scale, S, rtol=1e-12)
+    # strided column read at t = 0.7 (BinReader::read_prices_at_target_time)
+    j = int(round(0.7 / dt)) - 1
+    np.testing.assert_allclose(payload[:, j] * scale, S[:, j], rtol=1e-12)
+
+
+def test_paths_file_fp32_no_noise(qk, handle, tmp_path):
+    """NoNoiseTest through the .paths writer: every path at T equals S0 e^{(r-q)T} (FP32: 5e-3)."""
+    y = YAML.format(otype="European", right="Call", dist="false", greeks="false", prec="FP32", engine="batch",
+                    out_dir=str(tmp_path), paths="nn.paths")
+    y = y.replace("Variance: 0.04", "Variance: 0.0").replace("k: 2.0", "k: 0.0").replace("theta: 0.04", "theta: 0.0")
+    y = y.replace("sigma: 0.3", "sigma: 0.0").replace("rho: -0.7", "rho: 0.0")
+    cfg = qk.Parser.parse_string(y)
+    cfg.n_paths = 100
+    qk.MCDispatcher(cfg, handle).launch_montecarlo()
+    data = (tmp_path / "nn.paths").read_bytes()
+    assert struct.unpack_from("<i", data, 12)[0] == 4
+    payload = np.frombuffer(data, dtype=np.float32, offset=40).reshape(100, 128)
+    assert np.all(np.abs(payload[:, -1] * 100.0 - 100.0 * math.exp(0.03)) < 5e-3)
+
+
+def test_payoff_percentiles(qk, handle, oracle, tmp_path):
+    """OptionPricer::analyze_risk_neutral_discounted_payoff_distribution (OptionPricer.hpp:340-360)."""
+    cfg = _cfg(qk, tmp_path, otype="Asian", dist="true")
+    res = qk.MCDispatcher(cfg, handle).launch_montecarlo()
+    k, _ = cfg.to_contract()
+    pay = np.sort(oracle.payoffs(k))
+    eff = math.exp(-0.05 * 1.0) * 100.0
+    N = len(pay)
+    fr = [0.01, 0.05, 0.10, 0.20, 0.30, 0.40, 0.50, 0.60, 0.70, 0.80, 0.90, 0.95, 0.99]
+    want = [pay[0] * eff] + [pay[int(N * f)] * eff for f in fr] + [pay[-1] * eff]
+    got = list(res.OptionPrice.percentiles.values())
+    np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12)
+
+
+def test_cli_runs_a_config(qk, handle, tmp_path):
+    y = YAML.format(otype="BarrierUpAndOut", right="Call", dist="false", greeks="true", prec="FP32", engine="batch",
+                    out_dir=str(tmp_path), paths="")
+    p = tmp_path / "cfg.yaml"
+    p.write_text(y)
+    exe = ROOT / "quantkos_b200" / "quantkos"
+    out = subprocess.run([str(exe), str(p)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert "Estimated Option Price" in out.stdout and "Delta" in out.stdout
+    bad = subprocess.run([str(exe), str(tmp_path / "missing.yaml")], capture_output=True, text=True, timeout=60)
+    assert bad.returncode == 1 and "File not found" in bad.stderr
+
+
+def test_server_result_alone_equals_in_the_mix(qk, handle):
+    """Continuous batching: a request priced alone and the same request admitted together with
+    others (arriving while work is on the GPU) give identical results."""
+    from quantkos_b200 import workloads as W
+    _, contracts = W.serving_stream(96, seed=11)
+    contracts = [c for c in contracts]
+    for c in contracts:  # keep the test short
+        c.n_paths = min(c.n_paths, 200_000)
+    probe = contracts[17]
+    alone = qk.price_batch([probe], None, handle)[0]["legs"][0]
+    with qk.Server(handle, 0, 16) as srv:
+        tickets = [srv.submit(c) for c in contracts[:40]]
+        t_probe = srv.submit(probe)
+        tickets += [srv.submit(c) for c in contracts[40:]]
+        got = None
+        while got is None:
+            got = srv.poll(t_probe, 1000)
+        for t in tickets:
+            while srv.poll(t, 1000) is None:
+                pass
+        st = srv.stats()
+    leg = got["legs"][0]
+    assert leg["price"] == pytest.approx(alone["price"], rel=1e-12)
+    assert leg["std_error"] == pytest.approx(alone["std_error"], rel=1e-9)
+    assert st["completed"] == 97 and st["rejected"] == 0 and st["batches"] >= 2
+    assert st["p50_ms"] > 0 and st["p99_ms"] >= st["p50_ms"]
+
+
+def test_server_admission_rejects_oversized(qk, handle):
+    from quantkos_b200 import workloads as W
+    big = W.american_lsm(n_paths=4_000_000)
+    with qk.Server(handle, 64, 8) as srv:  # 64 MiB budget: the LSM slabs do not fit
+        with pytest.raises(RuntimeError, match="admission budget"):
+            srv.submit(big)
+        small = qk.make_contract(n_paths=10_000, n_steps=10)
+        t = srv.submit(small)
+        while srv.poll(t, 1000) is None:
+            pass
+        assert srv.stats()["rejected"] == 1
+
+
+def test_mixed_batch_sample_vs_closed_forms(qk, handle, oracle):
+    """European legs of the seeded mixed batch within 3 SE (+ discretisation allowance for Euler)
+    of the Gil-Pelaez price, priced together in one batch with all Greeks."""
+    from quantkos_b200 import workloads as W
+    batch = W.mixed_batch(256)
+    res = qk.price_batch(batch, W.batch_greeks(), handle)
+    checked = fails = 0
+    for c, r in zip(batch, res):
+        leg = r["legs"][0]
+        if c.payoffs[0].type != qk.EUROPEAN or c.scheme == qk.EULER:
+            continue
+        exact = oracle.exact_call(2 if c.model == qk.BATES else 1, c, 200.0 if c.model == qk.HESTON else 0.0)
+        if c.payoffs[0].right == qk.PUT:  # put-call parity
+            exact += c.payoffs[0].strike * math.exp(-c.r * c.T) - c.S0 * math.exp(-c.q * c.T)
+        checked += 1
+        if abs(leg["price"] - exact) > 3.0 * leg["std_error"] + 2e-3 * exact:
+            fails += 1
+    assert checked >= 20
+    assert fails <= max(1, checked // 50), (fails, checked)
+
+
+def test_config0_plain_fp64_vs_closed_form(qk, handle, oracle):
+    """Plain method on the plain-method case (Heston Euler, 1,048,576 x 252, FP64) within 3 SE of
+    the Gil-Pelaez price (the allowance covers the Euler bias at dt = 1/252, measured here against a
+    1008-step run)."""
+    from quantkos_b200 import workloads as W
+    c = W.plain_heston_euler()
+    r = qk.price_plain(c, None, handle)["legs"][0]
+    exact = oracle.exact_call(1, c, 200.0)
+    fine = qk.make_contract(**{f: getattr(c, f) for f in ("S0", "v0", "r", "q", "kappa", "theta", "sigma", "rho")},
+                            scheme=qk.EULER, T=1.0, n_steps=1008, n_paths=1_048_576, seed=42, precision=qk.FP64,
+                            payoffs=[qk.payoff(0, 0, 100.0)])
+    rf = qk.price_plain(fine, None, handle)["legs"][0]
+    bias = abs(r["price"] - rf["price"])
+    assert abs(r["price"] - exact) <= 3.0 * r["std_error"] + 2.0 * bias + 1e-3, (r, exact, rf)
+    assert abs(rf["price"] - exact) <= 3.0 * rf["std_error"] + 1e-3
