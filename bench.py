@@ -51,7 +51,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-sample-paths", type=int, default=1 << 16)
+    ap.add_argument("--cpu-sample-paths", type=int, default=1 << 16,
+                    help="reference arm: paths per timed step (each step is a bounded sample of the workload)")
+    ap.add_argument("--cpu-baseline-paths", type=int, default=1 << 21,
+                    help="cpu_baseline leg of our arm: paths of the one timed sample (about 10-30 s of CPU work)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--paths", type=int, default=N_PATHS,
@@ -454,7 +457,7 @@ def main() -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         try:
-            cpu = {k: v for k, v in cpu_reference_rate(args.cpu_sample_paths).items() if k != "seconds"}
+            cpu = {k: v for k, v in cpu_reference_rate(args.cpu_baseline_paths).items() if k != "seconds"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable", "sample": str(e)}
 

@@ -524,9 +524,11 @@ qk_status finish_timing(qk_handle *h, double path_steps) {
     QK_CUDA_TRY(cudaEventElapsedTime(&ms_all, h->ev_start, h->ev_end));
     QK_CUDA_TRY(cudaEventElapsedTime(&ms_paths, h->ev_paths0, h->ev_paths1));
     QK_CUDA_TRY(cudaEventElapsedTime(&ms_rest, h->ev_paths1, h->ev_end));
-    h->timing.device_ms = ms_all + h->lsm_ms;
-    h->timing.paths_ms = ms_paths + h->lsm_paths_ms;
-    h->timing.reduce_ms = ms_rest + (h->lsm_ms - h->lsm_paths_ms);
+    double lsm_paths = 0.0, lsm_sweep = 0.0;
+    if (h->lsm_jobs > 0) lsm_timing(h, &lsm_paths, &lsm_sweep);
+    h->timing.device_ms = ms_all;
+    h->timing.paths_ms = ms_paths + lsm_paths;
+    h->timing.reduce_ms = ms_all - ms_paths - lsm_paths;
     h->timing.launches = h->launches + h->lsm_launches;
     h->timing.path_steps = path_steps;
     h->timing.h2d_bytes = h->h2d_bytes;
@@ -542,6 +544,7 @@ qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const q
     if (s != QK_OK) return s;
     h->lsm_ms = h->lsm_paths_ms = 0.0;
     h->lsm_launches = 0;
+    h->lsm_jobs = 0;
     if ((s = run_plan(h, h->plan)) != QK_OK) return s;
     std::vector<Moments> lsm_moments;
     if (!h->plan.american.empty()) {
@@ -683,6 +686,7 @@ qk_status qk_batch_run(qk_handle *h) {
     if (!h || !h->prepared) return fail(QK_ERR_STATE, "qk_batch_run before qk_batch_prepare");
     h->lsm_ms = h->lsm_paths_ms = 0.0;
     h->lsm_launches = 0;
+    h->lsm_jobs = 0;
     const qk_status s = run_plan(h, h->plan);
     if (s != QK_OK) return s;
     QK_CUDA_TRY(cudaEventRecord(h->ev_end, h->stream));

@@ -75,6 +75,8 @@ struct qk_handle {
     int64_t h2d_bytes = 0, d2h_bytes = 0;
     double lsm_ms = 0.0, lsm_paths_ms = 0.0;
     int64_t lsm_launches = 0;
+    std::vector<cudaEvent_t> lsm_events;  // per LSM job: forward start, forward end, sweep end
+    size_t lsm_jobs = 0;
 };
 
 namespace qk {
@@ -97,5 +99,8 @@ qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &
 qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Moments> &moments);
 void assemble_lsm_results(qk_handle *h, const Plan &plan, const std::vector<Moments> &moments, qk_result *out);
 void lsm_release(qk_handle *h);
+qk_status lsm_events_ensure(qk_handle *h, size_t n);
+// Device time of the last call's LSM jobs: forward slab kernels and backward sweeps.
+void lsm_timing(qk_handle *h, double *paths_ms, double *sweep_ms);
 
 }  // namespace qk

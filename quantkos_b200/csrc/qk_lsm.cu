@@ -101,94 +101,6 @@ __device__ __forceinline__ double continuation(const double *c, R S, R v, R K, d
     return s;
 }
 
-// Backward sweep over one date pair.  init: cash flows start as the payoff at
-// date d_upd (maturity); otherwise the exercise decision of date d_upd is
-// applied with its solved coefficients.  Then, if d_gram >= 0, the ITM
-// regression sums of date d_gram are accumulated with Y = cf * disc.
-template <class R, int BASIS>
-__global__ void __launch_bounds__(kLsmBlock) lsm_sweep_kernel(LsmArgs a, const R *__restrict__ slab_S,
-                                                             const R *__restrict__ slab_v, R *__restrict__ cf,
-                                                             int d_upd, int init, int d_gram,
-                                                             const double *__restrict__ coeffs,
-                                                             const double *__restrict__ centre,
-                                                             double *__restrict__ block_sums) {
-    constexpr int NB = BasisTraits<BASIS>::NB;
-    constexpr int NSUM = Sums<NB>::NSUM;
-    const R K = static_cast<R>(a.K);
-    const R disc = static_cast<R>(a.disc);
-    double acc[NSUM];
-#pragma unroll
-    for (int j = 0; j < NSUM; ++j) acc[j] = 0.0;
-    double cu[NB];
-    double cxu = 0.0, cvu = 0.0, cxg = 0.0, cvg = 0.0;
-    if (!init) {
-#pragma unroll
-        for (int i = 0; i < NB; ++i) cu[i] = coeffs[d_upd * kMaxCoef + i];
-        cxu = centre[2 * d_upd];
-        cvu = centre[2 * d_upd + 1];
-    }
-    if (d_gram >= 0) {
-        cxg = centre[2 * d_gram];
-        cvg = centre[2 * d_gram + 1];
-    }
-    const bool use_v = BASIS == QK_LSM_POLY_SV;
-    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < a.N; i += stride) {
-        R c;
-        const R S = slab_S[static_cast<int64_t>(d_upd) * a.ld + i];
-        const R iv = lsm_intrinsic<R>(a.right, S, K);
-        if (init) {
-            c = iv;
-        } else {
-            c = cf[i];
-            const R disc_c = c * disc;
-            if (iv > R(0)) {
-                const R v = use_v ? slab_v[static_cast<int64_t>(d_upd) * a.ld + i] : R(0);
-                const double hold = continuation<R, BASIS>(cu, S, v, K, cxu, cvu);
-                c = (static_cast<double>(iv) > hold) ? iv : disc_c;
-            } else {
-                c = disc_c;
-            }
-        }
-        cf[i] = c;
-        if (d_gram >= 0) {
-            const R Sg = slab_S[static_cast<int64_t>(d_gram) * a.ld + i];
-            const R ivg = lsm_intrinsic<R>(a.right, Sg, K);
-            if (ivg > R(0)) {
-                const R vg = use_v ? slab_v[static_cast<int64_t>(d_gram) * a.ld + i] : R(0);
-                const R Y = c * disc;
-                R b[NB];
-                eval_basis<R, BASIS>(Sg, vg, K, cxg, cvg, b);
-                int j = 0;
-#pragma unroll
-                for (int r = 0; r < NB; ++r) {
-                    const double br = static_cast<double>(b[r]);
-#pragma unroll
-                    for (int q = r; q < NB; ++q) acc[j++] += br * static_cast<double>(b[q]);
-                }
-#pragma unroll
-                for (int r = 0; r < NB; ++r) acc[j++] += static_cast<double>(b[r]) * static_cast<double>(Y);
-                acc[j] += 1.0;
-            }
-        }
-    }
-    if (d_gram < 0) return;
-    // block reduction of the NSUM sums
-    __shared__ double s_red[kLsmBlock / 32][NSUM];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int j = 0; j < NSUM; ++j) {
-        const double v = warp_sum(acc[j]);
-        if (lane == 0) s_red[warp][j] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < NSUM) {
-        double t = 0.0;
-        for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red[w][threadIdx.x];
-        block_sums[static_cast<int64_t>(blockIdx.x) * NSUM + threadIdx.x] = t;
-    }
-}
-
 // ---------------------------------------------------------------- FP64 solves
 // Reference solve: Tikhonov 1e-8, Cholesky, 1e-14 pivot floor, mean fallback
 // (LSMAmerican.hpp:516-613).  Returns 0 on success, 2 on fallback.
@@ -372,24 +284,156 @@ __device__ int solve_scaled(const double *sums, double *c) {
     return 1;
 }
 
-// One block: reduce the block sums of a date in fixed order, then solve.
-template <int BASIS>
-__global__ void __launch_bounds__(32) lsm_solve_kernel(const double *__restrict__ block_sums, int nblocks, int d,
-                                                      double *__restrict__ coeffs, int *__restrict__ flags) {
+// Four consecutive slab entries (rows are 16-byte aligned: ld is a multiple of 4).
+__device__ __forceinline__ void load4(const float *p, float v[4]) {
+    const float4 q = *reinterpret_cast<const float4 *>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void load4(const double *p, double v[4]) {
+    const double2 a = *reinterpret_cast<const double2 *>(p);
+    const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void store4(float *p, const float v[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double *p, const double v[4]) {
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
+}
+
+// Backward sweep over one date pair.  init: cash flows start as the payoff at
+// date d_upd (maturity); otherwise the exercise decision of date d_upd is
+// applied with its solved coefficients.  Then, if d_gram >= 0, the ITM
+// regression sums of date d_gram are accumulated with Y = cf * disc, reduced per
+// block, and the last block to finish (counted on `done`) reduces all block sums
+// in a fixed order and solves date d_gram's coefficients — no separate launch and
+// no wait: every other block simply exits.  Each thread handles groups of four
+// consecutive paths with 16-byte loads.
+template <class R, int BASIS>
+__global__ void __launch_bounds__(kLsmBlock, 2) lsm_sweep_kernel(LsmArgs a, const R *__restrict__ slab_S,
+                                                             const R *__restrict__ slab_v, R *__restrict__ cf,
+                                                             int d_upd, int init, int d_gram,
+                                                             double *__restrict__ coeffs,
+                                                             const double *__restrict__ centre,
+                                                             double *__restrict__ block_sums,
+                                                             unsigned int *__restrict__ done, int *__restrict__ flags) {
     constexpr int NB = BasisTraits<BASIS>::NB;
     constexpr int NSUM = Sums<NB>::NSUM;
-    __shared__ double s_sum[NSUM];
+    const R K = static_cast<R>(a.K);
+    const R disc = static_cast<R>(a.disc);
+    double acc[NSUM];
+#pragma unroll
+    for (int j = 0; j < NSUM; ++j) acc[j] = 0.0;
+    double cu[NB];
+    double cxu = 0.0, cvu = 0.0, cxg = 0.0, cvg = 0.0;
+    if (!init) {
+#pragma unroll
+        for (int i = 0; i < NB; ++i) cu[i] = coeffs[d_upd * kMaxCoef + i];
+        cxu = centre[2 * d_upd];
+        cvu = centre[2 * d_upd + 1];
+    }
+    if (d_gram >= 0) {
+        cxg = centre[2 * d_gram];
+        cvg = centre[2 * d_gram + 1];
+    }
+    constexpr bool use_v = BASIS == QK_LSM_POLY_SV;
+    const int64_t groups = a.ld / 4;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    const R *Su = slab_S + static_cast<int64_t>(d_upd) * a.ld;
+    const R *Vu = use_v ? slab_v + static_cast<int64_t>(d_upd) * a.ld : nullptr;
+    const R *Sg = slab_S + static_cast<int64_t>(d_gram < 0 ? 0 : d_gram) * a.ld;
+    const R *Vg = use_v ? slab_v + static_cast<int64_t>(d_gram < 0 ? 0 : d_gram) * a.ld : nullptr;
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < groups; g += stride) {
+        const int64_t i0 = 4 * g;
+        R S4[4], c4[4], v4[4] = {R(0), R(0), R(0), R(0)};
+        load4(Su + i0, S4);
+        if (use_v) load4(Vu + i0, v4);
+        if (!init) load4(cf + i0, c4);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const R iv = lsm_intrinsic<R>(a.right, S4[k], K);
+            if (init) {
+                c4[k] = iv;
+            } else {
+                const R disc_c = c4[k] * disc;
+                if (iv > R(0)) {
+                    const double hold = continuation<R, BASIS>(cu, S4[k], v4[k], K, cxu, cvu);
+                    c4[k] = (static_cast<double>(iv) > hold) ? iv : disc_c;
+                } else {
+                    c4[k] = disc_c;
+                }
+            }
+        }
+        store4(cf + i0, c4);
+        if (d_gram >= 0) {
+            R Sg4[4], vg4[4] = {R(0), R(0), R(0), R(0)};
+            load4(Sg + i0, Sg4);
+            if (use_v) load4(Vg + i0, vg4);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const R ivg = lsm_intrinsic<R>(a.right, Sg4[k], K);
+                if (ivg > R(0) && i0 + k < a.N) {
+                    const R Y = c4[k] * disc;
+                    R b[NB];
+                    eval_basis<R, BASIS>(Sg4[k], vg4[k], K, cxg, cvg, b);
+                    int j = 0;
+#pragma unroll
+                    for (int r = 0; r < NB; ++r) {
+                        const double br = static_cast<double>(b[r]);
+#pragma unroll
+                        for (int q = r; q < NB; ++q) acc[j++] += br * static_cast<double>(b[q]);
+                    }
+#pragma unroll
+                    for (int r = 0; r < NB; ++r) acc[j++] += static_cast<double>(b[r]) * static_cast<double>(Y);
+                    acc[j] += 1.0;
+                }
+            }
+        }
+    }
+    if (d_gram < 0) return;
+    // block reduction of the NSUM sums
+    __shared__ double s_red[kLsmBlock / 32][NSUM];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NSUM; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) s_red[warp][j] = v;
+    }
+    __syncthreads();
     if (threadIdx.x < NSUM) {
         double t = 0.0;
-        for (int b = 0; b < nblocks; ++b) t += block_sums[static_cast<int64_t>(b) * NSUM + threadIdx.x];
-        s_sum[threadIdx.x] = t;
+        for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red[w][threadIdx.x];
+        block_sums[static_cast<int64_t>(blockIdx.x) * NSUM + threadIdx.x] = t;
+        __threadfence();  // this block's sums are visible device-wide before it is counted
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    // last block: fixed-order reduction of all block sums, then the FP64 solve
+    __threadfence();
+    __shared__ double s_part[kLsmBlock / 32][NSUM];
+    if (warp < kLsmBlock / 32 && lane < NSUM) {
+        double t = 0.0;
+        for (int b = warp; b < static_cast<int>(gridDim.x); b += kLsmBlock / 32)
+            t += __ldcg(block_sums + static_cast<int64_t>(b) * NSUM + lane);
+        s_part[warp][lane] = t;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+        double sums[NSUM];
+        for (int j = 0; j < NSUM; ++j) {
+            double t = 0.0;
+            for (int w = 0; w < kLsmBlock / 32; ++w) t += s_part[w][j];
+            sums[j] = t;
+        }
         double c[NB];
-        const int f = (BASIS == QK_LSM_LAGUERRE3) ? solve_reference<NB>(s_sum, c) : solve_scaled<NB>(s_sum, c);
-        for (int i = 0; i < kMaxCoef; ++i) coeffs[d * kMaxCoef + i] = i < NB ? c[i] : 0.0;
-        flags[d] = f;
+        const int f = (BASIS == QK_LSM_LAGUERRE3) ? solve_reference<NB>(sums, c) : solve_scaled<NB>(sums, c);
+        for (int i = 0; i < kMaxCoef; ++i) coeffs[d_gram * kMaxCoef + i] = i < NB ? c[i] : 0.0;
+        flags[d_gram] = f;
+        *done = 0u;  // ready for the next date
     }
 }
 
@@ -466,29 +510,53 @@ namespace {
 template <class R, int BASIS>
 cudaError_t enqueue_backward(cudaStream_t s, int grid, const LsmArgs &a, const R *S, const R *V, R *cf,
                              double *coeffs, int *flags, const double *centre, double *block_sums,
-                             Moments *block_moments, int64_t *launches) {
+                             unsigned int *done, Moments *block_moments, int64_t *launches) {
     const int D = a.n_dates;
     if (D == 1) {
         lsm_final_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, 1, coeffs, centre, block_moments);
         ++*launches;
         return cudaGetLastError();
     }
-    lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre, block_sums);
+    cudaError_t e = cudaMemsetAsync(done, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre, block_sums,
+                                                          done, flags);
     ++*launches;
     for (int d = D - 2; d >= 1; --d) {
-        lsm_solve_kernel<BASIS><<<1, 32, 0, s>>>(block_sums, grid, d, coeffs, flags);
-        lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, d, 0, d - 1, coeffs, centre, block_sums);
-        *launches += 2;
+        lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, d, 0, d - 1, coeffs, centre, block_sums,
+                                                              done, flags);
+        ++*launches;
     }
-    lsm_solve_kernel<BASIS><<<1, 32, 0, s>>>(block_sums, grid, 0, coeffs, flags);
     lsm_final_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, 0, coeffs, centre, block_moments);
-    *launches += 2;
+    ++*launches;
     return cudaGetLastError();
 }
 
 }  // namespace
 
+qk_status lsm_events_ensure(qk_handle *h, size_t n) {
+    while (h->lsm_events.size() < n) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(QK_ERR_CUDA, "LSM: cudaEventCreate failed");
+        h->lsm_events.push_back(e);
+    }
+    h->lsm_jobs = n / 3;
+    return QK_OK;
+}
+
+void lsm_timing(qk_handle *h, double *paths_ms, double *sweep_ms) {
+    *paths_ms = *sweep_ms = 0.0;
+    for (size_t k = 0; k < h->lsm_jobs; ++k) {
+        float a = 0.f, b = 0.f;
+        if (cudaEventElapsedTime(&a, h->lsm_events[3 * k], h->lsm_events[3 * k + 1]) == cudaSuccess) *paths_ms += a;
+        if (cudaEventElapsedTime(&b, h->lsm_events[3 * k + 1], h->lsm_events[3 * k + 2]) == cudaSuccess) *sweep_ms += b;
+    }
+}
+
 void lsm_release(qk_handle *h) {
+    for (cudaEvent_t e : h->lsm_events) cudaEventDestroy(e);
+    h->lsm_events.clear();
+    h->lsm_jobs = 0;
     LsmArena &L = h->lsm;
     L.slab_S.release();
     L.slab_v.release();
@@ -516,7 +584,7 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
             if (plain) b.precision = QK_FP64;
             jobs.push_back({b, i, role});
         }
-    const int grid = h->sm_count * 4;
+    const int grid = h->sm_count * 2;
     const size_t nj = jobs.size();
     qk_status st;
     // sizes
@@ -538,7 +606,8 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
     if ((st = L.cashflow.ensure(max_cf)) != QK_OK) return st;
     if ((st = L.block_sums.ensure(static_cast<size_t>(grid) * 64 * sizeof(double))) != QK_OK) return st;
     if ((st = L.coeffs.ensure(static_cast<size_t>(max_dates) * kMaxCoef * sizeof(double) + 2 * max_dates * sizeof(double) * nj + 64)) != QK_OK) return st;
-    if ((st = L.status.ensure(static_cast<size_t>(max_dates) * sizeof(int))) != QK_OK) return st;
+    if ((st = L.status.ensure(static_cast<size_t>(max_dates) * sizeof(int) + 256)) != QK_OK) return st;
+    if ((st = lsm_events_ensure(h, 3 * nj)) != QK_OK) return st;
     if ((st = L.task.ensure(nj * sizeof(TaskDev))) != QK_OK) return st;
     if ((st = h->d_lsm_moments.ensure(nj * grid * sizeof(Moments))) != QK_OK) return st;
     if ((st = h->h_lsm.ensure(nj * grid * sizeof(Moments))) != QK_OK) return st;
@@ -573,9 +642,11 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         const int prec = b.precision;
         const bool use_v = b.lsm_basis == QK_LSM_POLY_SV;
         // forward: exercise-date slabs
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k], h->stream));
         QK_CUDA_LSM(launch_slab_paths(prec, h->stream, static_cast<const TaskDev *>(L.task.ptr) + k, 0, b.n_paths,
                                       stride, L.slab_S.ptr, use_v ? L.slab_v.ptr : nullptr, ld));
         h->lsm_launches++;
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 1], h->stream));
         LsmArgs a;
         a.N = b.n_paths;
         a.ld = ld;
@@ -587,30 +658,33 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         const double *cen = d_centre + centre_off[k];
         double *bs = static_cast<double *>(L.block_sums.ptr);
         int *fl = static_cast<int *>(L.status.ptr);
+        unsigned int *done = reinterpret_cast<unsigned int *>(static_cast<char *>(L.status.ptr) +
+                                                              ((static_cast<size_t>(max_dates) * sizeof(int) + 127) / 128) * 128);
         cudaError_t e;
         if (prec == QK_FP32) {
             if (use_v)
                 e = enqueue_backward<float, QK_LSM_POLY_SV>(h->stream, grid, a, static_cast<const float *>(L.slab_S.ptr),
                                                            static_cast<const float *>(L.slab_v.ptr),
-                                                           static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, bm,
+                                                           static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, done, bm,
                                                            &h->lsm_launches);
             else
                 e = enqueue_backward<float, QK_LSM_LAGUERRE3>(h->stream, grid, a, static_cast<const float *>(L.slab_S.ptr),
                                                              nullptr, static_cast<float *>(L.cashflow.ptr), d_coeffs, fl,
-                                                             cen, bs, bm, &h->lsm_launches);
+                                                             cen, bs, done, bm, &h->lsm_launches);
         } else {
             if (use_v)
                 e = enqueue_backward<double, QK_LSM_POLY_SV>(h->stream, grid, a, static_cast<const double *>(L.slab_S.ptr),
                                                             static_cast<const double *>(L.slab_v.ptr),
                                                             static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen, bs,
-                                                            bm, &h->lsm_launches);
+                                                            done, bm, &h->lsm_launches);
             else
                 e = enqueue_backward<double, QK_LSM_LAGUERRE3>(h->stream, grid, a,
                                                               static_cast<const double *>(L.slab_S.ptr), nullptr,
                                                               static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen,
-                                                              bs, bm, &h->lsm_launches);
+                                                              bs, done, bm, &h->lsm_launches);
         }
         if (e != cudaSuccess) return fail(QK_ERR_CUDA, std::string("LSM launch: ") + cudaGetErrorString(e));
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 2], h->stream));
         LsmTaskInfo info;
         info.contract = jobs[k].contract;
         info.role = jobs[k].role;
