@@ -388,8 +388,9 @@ qk_status run_plan(qk_handle *h, Plan &plan) {
                 const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme);
                 const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
                 // one task: its own queue cursor, its own tile range (prefix of one task = itself)
+                const uint64_t seed = static_cast<uint64_t>(t.key0) | (static_cast<uint64_t>(t.key1) << 32);
                 QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
-                                               t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart));
+                                               t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed));
                 h->launches++;
             }
         } else {
@@ -404,8 +405,13 @@ qk_status run_plan(qk_handle *h, Plan &plan) {
                 const int64_t slots = slots_end - tb.tile_begin;
                 const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme);
                 const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
+                bool uniform_key = true;
+                for (size_t i = b; i < e; ++i)
+                    uniform_key &= plan.tasks[i].key0 == tb.key0 && plan.tasks[i].key1 == tb.key1;
+                const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
                 QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
-                                               static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart));
+                                               static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
+                                               uniform_key, seed));
                 h->launches++;
                 b = e;
             }
@@ -759,7 +765,7 @@ qk_status qk_paths_dump(qk_handle *h, const qk_contract *c, int64_t first, int64
     char *dS = base + ((sizeof(TaskDev) + 255) / 256) * 256;
     char *dv = dS + cells * esz;
     QK_CUDA_TRY(cudaMemcpyAsync(dt, &t, sizeof(TaskDev), cudaMemcpyHostToDevice, h->stream));
-    QK_CUDA_TRY(launch_slab_paths(prec, h->stream, dt, first, count, 1, dS, dv, count));
+    QK_CUDA_TRY(launch_slab_paths(prec, n.model, n.scheme, n.seed, h->stream, dt, first, count, 1, dS, dv, count));
     std::vector<char> hS(cells * esz), hv(cells * esz);
     QK_CUDA_TRY(cudaMemcpyAsync(hS.data(), dS, cells * esz, cudaMemcpyDeviceToHost, h->stream));
     QK_CUDA_TRY(cudaMemcpyAsync(hv.data(), dv, cells * esz, cudaMemcpyDeviceToHost, h->stream));

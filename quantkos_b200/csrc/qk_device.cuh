@@ -41,6 +41,34 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
     return c;
 }
 
+// Round keys k_r = (k0 + r W0, k1 + r W1), r = 0..9, precomputed on the host and
+// passed by value as a kernel parameter: the XORs then read them straight from
+// the parameter bank, with no key arithmetic per round.
+struct PhiloxRoundKeys {
+    uint32_t k[20];
+};
+
+inline PhiloxRoundKeys philox_round_keys(uint32_t k0, uint32_t k1) {
+    PhiloxRoundKeys rk;
+    for (int r = 0; r < 10; ++r) {
+        rk.k[2 * r] = k0 + static_cast<uint32_t>(r) * kPhiloxW0;
+        rk.k[2 * r + 1] = k1 + static_cast<uint32_t>(r) * kPhiloxW1;
+    }
+    return rk;
+}
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, const PhiloxRoundKeys &rk) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = static_cast<uint64_t>(kPhiloxM0) * c.x;
+        const uint64_t p1 = static_cast<uint64_t>(kPhiloxM1) * c.z;
+        const uint32_t lo0 = static_cast<uint32_t>(p0), hi0 = static_cast<uint32_t>(p0 >> 32);
+        const uint32_t lo1 = static_cast<uint32_t>(p1), hi1 = static_cast<uint32_t>(p1 >> 32);
+        c = U4{hi1 ^ c.y ^ rk.k[2 * r], lo1, hi0 ^ c.w ^ rk.k[2 * r + 1], lo0};
+    }
+    return c;
+}
+
 // ============================================================================
 // Arithmetic policy.  FP32 uses the SFU (MUFU) approximations explicitly;
 // FP64 uses the correctly-rounded / IEEE CUDA library functions.
@@ -236,23 +264,26 @@ __device__ __forceinline__ void step_qe(const StepConst<R> &p, R &S, R &v, R Zv,
         vn = R(0);
         logM = R(0);
     } else {
-        const R inv_m = Math<R>::rcp(m);
-        const R psi = s2 * inv_m * inv_m;
-        if (psi <= p.eps) {
+        // psi = s2 / m^2 is compared as s2 against eps m^2 and psi_c m^2 (m > 0)
+        const R m2 = m * m;
+        if (s2 <= p.eps * m2) {
             vn = m;
             logM = R(0);
-        } else if (psi <= p.psi_c) {
-            const R two_ip = Math<R>::div(R(2), psi);
+        } else if (s2 <= p.psi_c * m2) {
+            const R two_ip = R(2) * m2 * Math<R>::rcp(s2);  // 2 / psi
             const R b2 = two_ip - R(1) + Math<R>::sqrt(two_ip * (two_ip - R(1)));
-            const R a = Math<R>::div(m, R(1) + b2);
+            const R a = m * Math<R>::rcp(R(1) + b2);
             const R bz = Math<R>::sqrt(b2) + Zv;
             vn = a * bz * bz;
-            // 0.5/a = 0.5 (1 + b2) / m
-            const R safe_A = rmin(p.A, R(0.5) * (R(1) + b2) * inv_m - p.eps);
-            const R term = R(1) - R(2) * safe_A * a;
+            // min(A, 0.5/a - eps) enters only through its product with a > 0:
+            // safe_A a = min(A a, 0.5 - eps a)
+            const R Aa = rmin(p.A * a, R(0.5) - p.eps * a);
+            const R term = R(1) - R(2) * Aa;
             // M = exp(A b2 a / term) / sqrt(term)  =>  log M = A b2 a / term - log(term) / 2
-            logM = Math<R>::div(safe_A * b2 * a, term) - R(0.5) * Math<R>::log(term);
+            logM = Aa * b2 * Math<R>::rcp(term) - R(0.5) * Math<R>::log(term);
         } else {
+            const R inv_m = Math<R>::rcp(m);
+            const R psi = s2 * inv_m * inv_m;
             const R pz = Math<R>::div(psi - R(1), psi + R(1));
             const R beta = (R(1) - pz) * inv_m;
             const R U = R(0.5) * (R(1) + Math<R>::erf(Zv * p.inv_sqrt2));

@@ -14,13 +14,15 @@ constexpr int kWarpTilePaths = 32;  // paths per round of a warp tile (one per l
 #endif
 constexpr int kPathMinBlocksFp32 = QK_PATH_MIN_BLOCKS_FP32;  // resident blocks per SM the FP32 path kernel is register-budgeted for
 
+// uniform_key: every task of the launch has Philox key `seed` (round keys go in the
+// kernel parameters); otherwise each task's key is read from its descriptor.
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
-                               unsigned long long *cursor, Moments *partials);
+                               unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed);
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
                                TaskMoments *out);
-cudaError_t launch_slab_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t first_path, int64_t count,
-                              int stride, void *slab_S, void *slab_v, int64_t ld);
+cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t seed, cudaStream_t s, const TaskDev *task,
+                              int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld);
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
                               int umax, int n, double *S_out, double *v_out, int *status);
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);

@@ -116,7 +116,7 @@ extern "C" qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_res
     if (e == cudaSuccess) e = cudaMemsetAsync(d_cursor, 0, sizeof(unsigned long long), st);  // queue starts empty
     if (e == cudaSuccess)
         e = qk::launch_price_tiles(t.precision, t.model, t.scheme, std::max(grid, 1), st, d_task, d_prefix, 1, 0,
-                                   t.n_tiles, d_cursor, d_partials);
+                                   t.n_tiles, d_cursor, d_partials, true, c->seed);
     if (e == cudaSuccess) e = qk::launch_merge_tasks(1, st, d_task, d_partials, d_moments);
     if (e == cudaSuccess) e = cudaMemcpyAsync(m, d_moments, sizeof(m), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

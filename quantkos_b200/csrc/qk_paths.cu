@@ -55,6 +55,17 @@ __device__ __forceinline__ void track(PathState<R> &st, R &blk) {
     st.smin = rmin(st.smin, st.S);
 }
 
+// Philox with round keys read from the kernel's parameter bank (all tasks of the
+// launch share the seed) or computed per round from the task's key.
+struct ParamKeys {
+    const PhiloxRoundKeys &rk;
+    __device__ __forceinline__ U4 operator()(U4 c) const { return philox4x32_10(c, rk); }
+};
+struct RegKeys {
+    uint32_t k0, k1;
+    __device__ __forceinline__ U4 operator()(U4 c) const { return philox4x32_10(c, k0, k1); }
+};
+
 // The step's first Poisson uniform decides whether a jump happened (Knuth's loop
 // continues only if it is >= exp(-lambda dt)).  FP32 compares the word directly:
 // (w >> 9) >= kmin  <=>  u01(w) >= exp(-lambda dt) in float, kmin precomputed exactly.
@@ -82,9 +93,9 @@ __device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st
     }
 }
 
-template <class R, int MODEL, int SCHEME, class Sink>
-__device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0, int n_steps, uint32_t k0,
-                                              uint32_t k1, uint32_t path, uint32_t stream, uint32_t kmin,
+template <class R, int MODEL, int SCHEME, class Gen, class Sink>
+__device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
+                                              uint32_t k0, uint32_t k1, uint32_t path, uint32_t stream, uint32_t kmin,
                                               PathState<R> &st, const Sink &sink) {
     st.S = S0;
     st.v = v0;
@@ -97,9 +108,9 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
         U4 wp{0u, 0u, 0u, 0u};  // Poisson words of steps 4m .. 4m+3 (n0 is a multiple of 4)
         int n = n0;
         for (; n + 1 < n1; n += 2) {
-            const U4 w = philox4x32_10(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u}, k0, k1);
+            const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u});
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) wp = philox4x32_10(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u}, k0, k1);
+                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
             }
             const bool lo = (n & 3) == 0;
             one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, lo ? wp.x : wp.z, kmin, k0, k1, path, stream, n);
@@ -110,9 +121,9 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
             sink(n + 1, st.S, st.v);
         }
         if (n < n1) {
-            const U4 w = philox4x32_10(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u}, k0, k1);
+            const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u});
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) wp = philox4x32_10(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u}, k0, k1);
+                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
             }
             one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, (n & 3) == 0 ? wp.x : wp.z, kmin, k0, k1, path, stream, n);
             track(st, blk);
@@ -135,13 +146,14 @@ __device__ __forceinline__ void simulate_dispatch(const TaskDev &t, const StepCo
     const R S0 = static_cast<R>(t.S0);
     const R v0 = static_cast<R>(t.v0);
     const uint32_t km = t.jump_kmin;
+    const RegKeys g{t.key0, t.key1};
     switch (t.model * 3 + t.scheme) {
-        case 0: simulate_path<R, kHeston, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
-        case 1: simulate_path<R, kHeston, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
-        case 2: simulate_path<R, kHeston, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
-        case 3: simulate_path<R, kBates, kEuler>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
-        case 4: simulate_path<R, kBates, kMilstein>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
-        default: simulate_path<R, kBates, kQE>(p, S0, v0, t.n_steps, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 0: simulate_path<R, kHeston, kEuler>(p, S0, v0, t.n_steps, g, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 1: simulate_path<R, kHeston, kMilstein>(p, S0, v0, t.n_steps, g, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 2: simulate_path<R, kHeston, kQE>(p, S0, v0, t.n_steps, g, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 3: simulate_path<R, kBates, kEuler>(p, S0, v0, t.n_steps, g, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        case 4: simulate_path<R, kBates, kMilstein>(p, S0, v0, t.n_steps, g, t.key0, t.key1, path, t.stream, km, st, sink); break;
+        default: simulate_path<R, kBates, kQE>(p, S0, v0, t.n_steps, g, t.key0, t.key1, path, t.stream, km, st, sink); break;
     }
 }
 
@@ -164,11 +176,11 @@ __device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int
     return lo;
 }
 
-template <class R, int MODEL, int SCHEME>
+template <class R, int MODEL, int SCHEME, bool UK>
 __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp32 : 1)
     price_tiles_kernel(const TaskDev *__restrict__ tasks, const int64_t *__restrict__ prefix, int32_t n_tasks,
                        int64_t slot_begin, int64_t slot_end, unsigned long long *__restrict__ cursor,
-                       Moments *__restrict__ partials) {
+                       Moments *__restrict__ partials, const PhiloxRoundKeys rk) {
     // Every warp is an independent worker: it pops a tile (kWarpTilePaths * ppt paths of one
     // task), keeps the tile's running moments per leg in its own shared-memory slots and
     // writes one record per leg.  No block-wide barrier anywhere.
@@ -206,8 +218,13 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
             const bool active = path < n_paths;
             PathState<R> st;
             if (active) {
-                simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, k0, k1, static_cast<uint32_t>(path), stream, kmin,
-                                                st, NoSink{});
+                if constexpr (UK) {
+                    simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
+                                                    static_cast<uint32_t>(path), stream, kmin, st, NoSink{});
+                } else {
+                    simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
+                                                    static_cast<uint32_t>(path), stream, kmin, st, NoSink{});
+                }
             } else {
                 st.S = st.smax = st.smin = R(0);
                 st.ssum = 0.0;
@@ -227,18 +244,23 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
 
 template <class R>
 using PriceKernel = void (*)(const TaskDev *, const int64_t *, int32_t, int64_t, int64_t, unsigned long long *,
-                             Moments *);
+                             Moments *, const PhiloxRoundKeys);
+
+template <class R, bool UK>
+__host__ PriceKernel<R> price_kernel_for_keys(int model, int scheme) {
+    switch (model * 3 + scheme) {
+        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK>;
+        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK>;
+        case 2: return price_tiles_kernel<R, kHeston, kQE, UK>;
+        case 3: return price_tiles_kernel<R, kBates, kEuler, UK>;
+        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK>;
+        default: return price_tiles_kernel<R, kBates, kQE, UK>;
+    }
+}
 
 template <class R>
-__host__ PriceKernel<R> price_kernel_for(int model, int scheme) {
-    switch (model * 3 + scheme) {
-        case 0: return price_tiles_kernel<R, kHeston, kEuler>;
-        case 1: return price_tiles_kernel<R, kHeston, kMilstein>;
-        case 2: return price_tiles_kernel<R, kHeston, kQE>;
-        case 3: return price_tiles_kernel<R, kBates, kEuler>;
-        case 4: return price_tiles_kernel<R, kBates, kMilstein>;
-        default: return price_tiles_kernel<R, kBates, kQE>;
-    }
+__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true) {
+    return uniform_key ? price_kernel_for_keys<R, true>(model, scheme) : price_kernel_for_keys<R, false>(model, scheme);
 }
 
 // Per task and leg: merge the task's tile moments (Chan updates, strided per
@@ -267,18 +289,37 @@ __global__ void __launch_bounds__(256) merge_tasks_kernel(const TaskDev *__restr
 }
 
 // Exercise-date slabs (LSM) / full path dump: one path per thread, S (and v)
-// after every `stride`-th step stored as SoA rows slab[date][path].
-template <class R>
+// after every `stride`-th step stored as SoA rows slab[date][path] (coalesced:
+// consecutive threads write consecutive columns).  Specialised per kind, with the
+// Philox round keys in the kernel parameters.
+template <class R, int MODEL, int SCHEME>
 __global__ void __launch_bounds__(kPathBlock) slab_paths_kernel(const TaskDev *__restrict__ task, int64_t first_path,
                                                                int64_t count, int stride, R *__restrict__ slab_S,
-                                                               R *__restrict__ slab_v, int64_t ld) {
+                                                               R *__restrict__ slab_v, int64_t ld,
+                                                               const PhiloxRoundKeys rk) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const TaskDev &t = *task;
     const StepConst<R> p = task_const<R>(t);
     SlabSink<R> sink{slab_S, slab_v, ld, i, stride};
     PathState<R> st;
-    simulate_dispatch<R>(t, p, static_cast<uint32_t>(first_path + i), st, sink);
+    simulate_path<R, MODEL, SCHEME>(p, static_cast<R>(t.S0), static_cast<R>(t.v0), t.n_steps, ParamKeys{rk}, t.key0,
+                                    t.key1, static_cast<uint32_t>(first_path + i), t.stream, t.jump_kmin, st, sink);
+}
+
+template <class R>
+using SlabKernel = void (*)(const TaskDev *, int64_t, int64_t, int, R *, R *, int64_t, const PhiloxRoundKeys);
+
+template <class R>
+SlabKernel<R> slab_kernel_for(int model, int scheme) {
+    switch (model * 3 + scheme) {
+        case 0: return slab_paths_kernel<R, kHeston, kEuler>;
+        case 1: return slab_paths_kernel<R, kHeston, kMilstein>;
+        case 2: return slab_paths_kernel<R, kHeston, kQE>;
+        case 3: return slab_paths_kernel<R, kBates, kEuler>;
+        case 4: return slab_paths_kernel<R, kBates, kMilstein>;
+        default: return slab_paths_kernel<R, kBates, kQE>;
+    }
 }
 
 // Per-path payoff of leg 0 (undiscounted, normalised units), for the payoff
@@ -330,13 +371,15 @@ __global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double
 // ----------------------------------------------------------------------------
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
-                               unsigned long long *cursor, Moments *partials) {
+                               unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed) {
+    const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
+                                                 static_cast<uint32_t>(seed >> 32));
     if (precision == QK_FP32)
-        price_kernel_for<float>(model, scheme)<<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin,
-                                                                           slot_end, cursor, partials);
+        price_kernel_for<float>(model, scheme, uniform_key)<<<grid, kPathBlock, 0, s>>>(
+            tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     else
-        price_kernel_for<double>(model, scheme)<<<grid, kPathBlock, 0, s>>>(tasks, prefix, n_tasks, slot_begin,
-                                                                            slot_end, cursor, partials);
+        price_kernel_for<double>(model, scheme, uniform_key)<<<grid, kPathBlock, 0, s>>>(
+            tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     return cudaGetLastError();
 }
 
@@ -346,15 +389,17 @@ cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks
     return cudaGetLastError();
 }
 
-cudaError_t launch_slab_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t first_path, int64_t count,
-                              int stride, void *slab_S, void *slab_v, int64_t ld) {
+cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t seed, cudaStream_t s, const TaskDev *task,
+                              int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld) {
     const int64_t blocks = (count + kPathBlock - 1) / kPathBlock;
+    const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
+                                                 static_cast<uint32_t>(seed >> 32));
     if (precision == QK_FP32)
-        slab_paths_kernel<float><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
-            task, first_path, count, stride, static_cast<float *>(slab_S), static_cast<float *>(slab_v), ld);
+        slab_kernel_for<float>(model, scheme)<<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
+            task, first_path, count, stride, static_cast<float *>(slab_S), static_cast<float *>(slab_v), ld, rk);
     else
-        slab_paths_kernel<double><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
-            task, first_path, count, stride, static_cast<double *>(slab_S), static_cast<double *>(slab_v), ld);
+        slab_kernel_for<double>(model, scheme)<<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
+            task, first_path, count, stride, static_cast<double *>(slab_S), static_cast<double *>(slab_v), ld, rk);
     return cudaGetLastError();
 }
 
