@@ -179,8 +179,11 @@ qk_status qk_price_plain(qk_handle *h, const qk_contract *c, const qk_greeks *g,
 qk_status qk_price_batch(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g, qk_result *out);
 
 /* Device-resident form of qk_price_batch for callers that reprice the same set:
- * prepare uploads the task/tile descriptors once, run queues the kernels
- * (asynchronously, on the handle's stream), fetch waits and fills `out`. */
+ * prepare uploads the task/tile descriptors once and captures the steady launch
+ * sequence (queue reset, path kernels, merge, copy of the moments to the host)
+ * in a CUDA graph; run replays the graph (asynchronously, on the handle's
+ * stream), fetch waits and fills `out`.  Any other pricing call on the handle
+ * drops the prepared set (run then returns QK_ERR_STATE). */
 qk_status qk_batch_prepare(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g);
 qk_status qk_batch_run(qk_handle *h);
 qk_status qk_batch_fetch(qk_handle *h, qk_result *out, int32_t n);

@@ -352,9 +352,87 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     return QK_OK;
 }
 
-// Upload the plan and queue its kernels.  Tasks of one precision form one
-// persistent launch (the batched engine) or, for the plain method, every task
-// is its own launch.
+// Device arenas for the plan and the copy of its task descriptors and tile
+// prefix to the device.
+static qk_status upload_plan(qk_handle *h, const Plan &plan) {
+    const size_t nt = plan.tasks.size();
+    qk_status s;
+    if ((s = h->d_tasks.ensure(nt * sizeof(TaskDev))) != QK_OK) return s;
+    if ((s = h->d_prefix.ensure(nt * sizeof(int64_t))) != QK_OK) return s;
+    if ((s = h->d_partials.ensure(static_cast<size_t>(plan.total_records) * sizeof(Moments))) != QK_OK) return s;
+    if ((s = h->d_moments.ensure(nt * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK) return s;
+    if ((s = h->d_cursor.ensure(nt * sizeof(unsigned long long))) != QK_OK) return s;
+    if ((s = h->h_tasks.ensure(nt * sizeof(TaskDev) + nt * sizeof(int64_t))) != QK_OK) return s;
+    if ((s = h->h_moments.ensure(nt * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK) return s;
+    TaskDev *ht = static_cast<TaskDev *>(h->h_tasks.ptr);
+    int64_t *hp = reinterpret_cast<int64_t *>(ht + nt);
+    std::memcpy(ht, plan.tasks.data(), nt * sizeof(TaskDev));
+    for (size_t i = 0; i < nt; ++i) hp[i] = plan.tasks[i].tile_begin;
+    QK_CUDA_TRY(cudaMemcpyAsync(h->d_tasks.ptr, ht, nt * sizeof(TaskDev), cudaMemcpyHostToDevice, h->stream));
+    QK_CUDA_TRY(cudaMemcpyAsync(h->d_prefix.ptr, hp, nt * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    return QK_OK;
+}
+
+// The steady part of a run: clear the queue cursors, launch the path kernels
+// (one persistent launch per kernel kind for the batched engine, one launch per
+// task for the plain method), merge the tile moments and copy them to the host.
+// `capture`: the stream is being captured into a graph, so the timing events
+// are recorded as external event nodes of that graph.
+static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
+    const size_t nt = plan.tasks.size();
+    const unsigned ev_flags = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+    QK_CUDA_TRY(cudaMemsetAsync(h->d_cursor.ptr, 0, nt * sizeof(unsigned long long), h->stream));
+    QK_CUDA_TRY(cudaEventRecordWithFlags(h->ev_paths0, h->stream, ev_flags));
+    const TaskDev *dt = static_cast<const TaskDev *>(h->d_tasks.ptr);
+    const int64_t *dp = static_cast<const int64_t *>(h->d_prefix.ptr);
+    unsigned long long *dc = static_cast<unsigned long long *>(h->d_cursor.ptr);
+    Moments *dpart = static_cast<Moments *>(h->d_partials.ptr);
+    if (plan.plain) {
+        for (size_t i = 0; i < nt; ++i) {
+            const TaskDev &t = plan.tasks[i];
+            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme);
+            const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
+            // one task: its own queue cursor, its own tile range (prefix of one task = itself)
+            const uint64_t seed = static_cast<uint64_t>(t.key0) | (static_cast<uint64_t>(t.key1) << 32);
+            QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
+                                           t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed));
+            h->launches++;
+        }
+    } else {
+        size_t b = 0;
+        while (b < nt) {
+            size_t e = b;
+            const TaskDev &tb = plan.tasks[b];
+            while (e < nt && plan.tasks[e].precision == tb.precision && plan.tasks[e].model == tb.model &&
+                   plan.tasks[e].scheme == tb.scheme)
+                ++e;
+            const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
+            const int64_t slots = slots_end - tb.tile_begin;
+            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme);
+            const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
+            bool uniform_key = true;
+            for (size_t i = b; i < e; ++i)
+                uniform_key &= plan.tasks[i].key0 == tb.key0 && plan.tasks[i].key1 == tb.key1;
+            const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
+            QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
+                                           static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
+                                           uniform_key, seed));
+            h->launches++;
+            b = e;
+        }
+    }
+    QK_CUDA_TRY(cudaEventRecordWithFlags(h->ev_paths1, h->stream, ev_flags));
+    int64_t max_tiles = 0;
+    for (const TaskDev &t : plan.tasks) max_tiles = std::max<int64_t>(max_tiles, t.n_tiles);
+    QK_CUDA_TRY(launch_merge_tasks(static_cast<int>(nt), h->stream, dt, dpart,
+                                   static_cast<Moments *>(h->d_moments.ptr), max_tiles));
+    h->launches++;
+    QK_CUDA_TRY(cudaMemcpyAsync(h->h_moments.ptr, h->d_moments.ptr, nt * QK_MAX_PAYOFFS * sizeof(Moments),
+                                cudaMemcpyDeviceToHost, h->stream));
+    return QK_OK;
+}
+
+// Upload the plan and queue its kernels.
 qk_status run_plan(qk_handle *h, Plan &plan) {
     const size_t nt = plan.tasks.size();
     h->launches = 0;
@@ -362,69 +440,48 @@ qk_status run_plan(qk_handle *h, Plan &plan) {
     h->d2h_bytes = static_cast<int64_t>(nt * QK_MAX_PAYOFFS * sizeof(Moments));
     QK_CUDA_TRY(cudaEventRecord(h->ev_start, h->stream));
     if (nt > 0) {
-        qk_status s;
-        if ((s = h->d_tasks.ensure(nt * sizeof(TaskDev))) != QK_OK) return s;
-        if ((s = h->d_prefix.ensure(nt * sizeof(int64_t))) != QK_OK) return s;
-        if ((s = h->d_partials.ensure(static_cast<size_t>(plan.total_records) * sizeof(Moments))) != QK_OK) return s;
-        if ((s = h->d_moments.ensure(nt * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK) return s;
-        if ((s = h->d_cursor.ensure(nt * sizeof(unsigned long long))) != QK_OK) return s;
-        if ((s = h->h_tasks.ensure(nt * sizeof(TaskDev) + nt * sizeof(int64_t))) != QK_OK) return s;
-        if ((s = h->h_moments.ensure(nt * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK) return s;
-        TaskDev *ht = static_cast<TaskDev *>(h->h_tasks.ptr);
-        int64_t *hp = reinterpret_cast<int64_t *>(ht + nt);
-        std::memcpy(ht, plan.tasks.data(), nt * sizeof(TaskDev));
-        for (size_t i = 0; i < nt; ++i) hp[i] = plan.tasks[i].tile_begin;
-        QK_CUDA_TRY(cudaMemcpyAsync(h->d_tasks.ptr, ht, nt * sizeof(TaskDev), cudaMemcpyHostToDevice, h->stream));
-        QK_CUDA_TRY(cudaMemcpyAsync(h->d_prefix.ptr, hp, nt * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
-        QK_CUDA_TRY(cudaMemsetAsync(h->d_cursor.ptr, 0, nt * sizeof(unsigned long long), h->stream));
-        QK_CUDA_TRY(cudaEventRecord(h->ev_paths0, h->stream));
-        const TaskDev *dt = static_cast<const TaskDev *>(h->d_tasks.ptr);
-        const int64_t *dp = static_cast<const int64_t *>(h->d_prefix.ptr);
-        unsigned long long *dc = static_cast<unsigned long long *>(h->d_cursor.ptr);
-        Moments *dpart = static_cast<Moments *>(h->d_partials.ptr);
-        if (plan.plain) {
-            for (size_t i = 0; i < nt; ++i) {
-                const TaskDev &t = plan.tasks[i];
-                const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme);
-                const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
-                // one task: its own queue cursor, its own tile range (prefix of one task = itself)
-                const uint64_t seed = static_cast<uint64_t>(t.key0) | (static_cast<uint64_t>(t.key1) << 32);
-                QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
-                                               t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed));
-                h->launches++;
-            }
-        } else {
-            size_t b = 0;
-            while (b < nt) {
-                size_t e = b;
-                const TaskDev &tb = plan.tasks[b];
-                while (e < nt && plan.tasks[e].precision == tb.precision && plan.tasks[e].model == tb.model &&
-                       plan.tasks[e].scheme == tb.scheme)
-                    ++e;
-                const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
-                const int64_t slots = slots_end - tb.tile_begin;
-                const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme);
-                const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
-                bool uniform_key = true;
-                for (size_t i = b; i < e; ++i)
-                    uniform_key &= plan.tasks[i].key0 == tb.key0 && plan.tasks[i].key1 == tb.key1;
-                const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
-                QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
-                                               static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
-                                               uniform_key, seed));
-                h->launches++;
-                b = e;
-            }
-        }
-        QK_CUDA_TRY(cudaEventRecord(h->ev_paths1, h->stream));
-        QK_CUDA_TRY(launch_merge_tasks(static_cast<int>(nt), h->stream, dt, dpart, static_cast<Moments *>(h->d_moments.ptr)));
-        h->launches++;
-        QK_CUDA_TRY(cudaMemcpyAsync(h->h_moments.ptr, h->d_moments.ptr, nt * QK_MAX_PAYOFFS * sizeof(Moments),
-                                    cudaMemcpyDeviceToHost, h->stream));
-    } else {
-        QK_CUDA_TRY(cudaEventRecord(h->ev_paths0, h->stream));
-        QK_CUDA_TRY(cudaEventRecord(h->ev_paths1, h->stream));
+        qk_status s = upload_plan(h, plan);
+        if (s != QK_OK) return s;
+        return enqueue_plan(h, plan, false);
     }
+    QK_CUDA_TRY(cudaEventRecord(h->ev_paths0, h->stream));
+    QK_CUDA_TRY(cudaEventRecord(h->ev_paths1, h->stream));
+    return QK_OK;
+}
+
+void release_prepared(qk_handle *h) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graph_launches = 0;
+    h->prepared = false;
+}
+
+// Capture the prepared plan's steady sequence (enqueue_plan) into a graph; the
+// descriptors are uploaded once, before the capture, and stay on the device.
+static qk_status capture_prepared(qk_handle *h) {
+    Plan &plan = h->plan;
+    qk_status s = upload_plan(h, plan);
+    if (s != QK_OK) return s;
+    QK_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    QK_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->launches = 0;
+    s = enqueue_plan(h, plan, true);
+    const std::string err = s != QK_OK ? g_last_error : std::string();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+    if (s != QK_OK || ec != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return fail(s != QK_OK ? s : QK_ERR_CUDA,
+                    "qk_batch_prepare: graph capture failed: " + (s != QK_OK ? err : std::string(cudaGetErrorString(ec))));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        h->graph = nullptr;
+        return fail(QK_ERR_CUDA, std::string("qk_batch_prepare: cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+    }
+    h->graph_launches = h->launches;
     return QK_OK;
 }
 
@@ -546,6 +603,7 @@ qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const q
                               bool plain) {
     if (!h || !c || !out || n < 0) return fail(QK_ERR_INVALID_ARG, "NULL argument or negative count");
     QK_CUDA_TRY(cudaSetDevice(h->device));
+    release_prepared(h);  // the plan and arenas are about to change
     qk_status s = build_plan(h, c, n, gs, plain, h->plan);
     if (s != QK_OK) return s;
     h->lsm_ms = h->lsm_paths_ms = 0.0;
@@ -606,6 +664,7 @@ qk_status qk_destroy(qk_handle *h) {
     if (!h) return QK_OK;
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
+    release_prepared(h);
     lsm_release(h);
     h->d_tasks.release();
     h->d_prefix.release();
@@ -680,21 +739,34 @@ qk_status qk_price_batch(qk_handle *h, const qk_contract *c, int32_t n, const qk
 qk_status qk_batch_prepare(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g) {
     if (!h || !c || n < 0) return fail(QK_ERR_INVALID_ARG, "NULL argument or negative count");
     QK_CUDA_TRY(cudaSetDevice(h->device));
+    release_prepared(h);
     const auto gs = repeat_greeks(g, n);
     qk_status s = build_plan(h, c, n, gs.data(), false, h->plan);
     if (s != QK_OK) return s;
     if (!h->plan.american.empty()) return fail(QK_ERR_UNSUPPORTED, "qk_batch_prepare: American contracts go through qk_price_batch");
+    if (!h->plan.tasks.empty() && (s = capture_prepared(h)) != QK_OK) return s;
     h->prepared = true;
     return QK_OK;
 }
 
 qk_status qk_batch_run(qk_handle *h) {
     if (!h || !h->prepared) return fail(QK_ERR_STATE, "qk_batch_run before qk_batch_prepare");
+    QK_CUDA_TRY(cudaSetDevice(h->device));
     h->lsm_ms = h->lsm_paths_ms = 0.0;
     h->lsm_launches = 0;
     h->lsm_jobs = 0;
-    const qk_status s = run_plan(h, h->plan);
-    if (s != QK_OK) return s;
+    const size_t nt = h->plan.tasks.size();
+    h->h2d_bytes = 0;  // descriptors stay on the device between runs
+    h->d2h_bytes = static_cast<int64_t>(nt * QK_MAX_PAYOFFS * sizeof(Moments));
+    QK_CUDA_TRY(cudaEventRecord(h->ev_start, h->stream));
+    if (h->graph) {
+        QK_CUDA_TRY(cudaGraphLaunch(h->graph, h->stream));
+        h->launches = h->graph_launches;
+    } else {
+        QK_CUDA_TRY(cudaEventRecord(h->ev_paths0, h->stream));
+        QK_CUDA_TRY(cudaEventRecord(h->ev_paths1, h->stream));
+        h->launches = 0;
+    }
     QK_CUDA_TRY(cudaEventRecord(h->ev_end, h->stream));
     return QK_OK;
 }

@@ -110,9 +110,12 @@ struct Math<float> {
     static __device__ __forceinline__ float rcp(float x) { return ptx_rcp(x); }
     static __device__ __forceinline__ float div(float a, float b) { return a * ptx_rcp(b); }
     static __device__ __forceinline__ float erf(float x) { return erff(x); }
-    // uniform in (0,1): (k + 1/2) / 2^23, k = top 23 bits of the word
+    // uniform in (0,1): (k + 1/2) / 2^23, k = top 23 bits of the word.  The float
+    // 1 + k 2^-23 is built from its bits (k as the mantissa) and 1 - 2^-24 subtracted;
+    // both are exact and so is the difference (2k + 1) 2^-24, so this equals
+    // k * 2^-23 + 2^-24 bit for bit without an integer-to-float conversion.
     static __device__ __forceinline__ float u01(uint32_t w) {
-        return __fmaf_rn(static_cast<float>(w >> 9), 1.0f / 8388608.0f, 1.0f / 16777216.0f);
+        return __fsub_rn(__uint_as_float(0x3F800000u | (w >> 9)), 0.99999994039535522f);
     }
     // Box-Muller pair: R = sqrt(-2 ln u1), angle = 2*pi*(u2 - 1/2)
     static __device__ __forceinline__ void box_muller(uint32_t w1, uint32_t w2, float &z1, float &z2) {

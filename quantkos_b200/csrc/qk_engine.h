@@ -70,6 +70,8 @@ struct qk_handle {
     qk::LsmArena lsm;
     qk::Plan plan;
     bool prepared = false;
+    cudaGraphExec_t graph = nullptr;  // the prepared batch's launch sequence (qk_batch_prepare)
+    int64_t graph_launches = 0;
     qk_timing timing{};
     int64_t launches = 0;
     int64_t h2d_bytes = 0, d2h_bytes = 0;
@@ -102,5 +104,7 @@ void lsm_release(qk_handle *h);
 qk_status lsm_events_ensure(qk_handle *h, size_t n);
 // Device time of the last call's LSM jobs: forward slab kernels and backward sweeps.
 void lsm_timing(qk_handle *h, double *paths_ms, double *sweep_ms);
+// Drop the prepared batch (its graph holds pointers into the handle's arenas).
+void release_prepared(qk_handle *h);
 
 }  // namespace qk

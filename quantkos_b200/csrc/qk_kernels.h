@@ -19,8 +19,9 @@ constexpr int kPathMinBlocksFp32 = QK_PATH_MIN_BLOCKS_FP32;  // resident blocks 
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
                                unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed);
+// max_tiles: the largest n_tiles among the tasks (sets the block width).
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
-                               TaskMoments *out);
+                               TaskMoments *out, int64_t max_tiles = 0);
 cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t seed, cudaStream_t s, const TaskDev *task,
                               int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld);
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,

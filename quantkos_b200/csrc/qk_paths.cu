@@ -263,28 +263,70 @@ __host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key
     return uniform_key ? price_kernel_for_keys<R, true>(model, scheme) : price_kernel_for_keys<R, false>(model, scheme);
 }
 
-// Per task and leg: merge the task's tile moments (Chan updates, strided per
-// thread, then a fixed-shape tree), deterministic for a given tile plan.
-__global__ void __launch_bounds__(256) merge_tasks_kernel(const TaskDev *__restrict__ tasks,
-                                                          const Moments *__restrict__ partials,
-                                                          TaskMoments *__restrict__ out) {
-    __shared__ Moments s[256];
+// Per task and leg: merge the task's tile moments in one pass about a shift c
+// (the first tile's mean).  With d_i = mean_i - c:  N = sum n_i,  D = sum n_i d_i,
+// Q = sum (M2_i + n_i d_i^2), then mean = c + D / N and M2 = Q - D^2 / N (the
+// pairwise update of Chan et al. applied to all tiles at once; c lies within a
+// few standard errors of the mean, so D^2 / N is a small correction to Q).  No
+// division per record; per-thread sums fold through a fixed-shape tree, so the
+// result is deterministic for a given tile plan.
+__device__ __forceinline__ void block_sum4(double &a, double &b, double &c, double &d, double (*red)[32]) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    d = warp_sum(d);
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+        red[2][warp] = c;
+        red[3][warp] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a = b = c = d = 0.0;
+        for (int w = 0; w < nw; ++w) {
+            a += red[0][w];
+            b += red[1][w];
+            c += red[2][w];
+            d += red[3][w];
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(1024) merge_tasks_kernel(const TaskDev *__restrict__ tasks,
+                                                           const Moments *__restrict__ partials,
+                                                           TaskMoments *__restrict__ out) {
+    __shared__ double red[4][32];
     const TaskDev &t = tasks[blockIdx.x];
-    for (int k = 0; k < t.n_payoffs; ++k) {
-        Moments acc{0.0, 0.0, 0.0, 0.0};
-        for (int i = threadIdx.x; i < t.n_tiles; i += blockDim.x)
-            acc = chan_merge(acc, partials[t.partial_base + static_cast<int64_t>(i) * t.n_payoffs + k]);
-        s[threadIdx.x] = acc;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (static_cast<int>(threadIdx.x) < w) s[threadIdx.x] = chan_merge(s[threadIdx.x], s[threadIdx.x + w]);
-            __syncthreads();
+    const int np = t.n_payoffs;
+    const int64_t n_tiles = t.n_tiles;
+    const Moments *rec = partials + t.partial_base;
+    for (int k = 0; k < np; ++k) {
+        const double c = n_tiles > 0 ? rec[k].mean : 0.0;
+        double n = 0.0, D = 0.0, Q = 0.0, itm = 0.0;
+        for (int64_t i = threadIdx.x; i < n_tiles; i += blockDim.x) {
+            const Moments m = rec[i * np + k];
+            const double d = m.mean - c;
+            const double nd = m.n * d;
+            n += m.n;
+            D += nd;
+            Q += fma(nd, d, m.m2);
+            itm += m.itm;
         }
+        block_sum4(n, D, Q, itm, red);
         if (threadIdx.x == 0) {
-            const Moments m = s[0];
-            out[static_cast<int64_t>(blockIdx.x) * QK_MAX_PAYOFFS + k] = m;
+            Moments r{0.0, 0.0, 0.0, 0.0};
+            if (n > 0.0) {
+                r.n = n;
+                r.mean = c + D / n;
+                r.m2 = fmax(Q - D * (D / n), 0.0);
+                r.itm = itm;
+            }
+            out[static_cast<int64_t>(blockIdx.x) * QK_MAX_PAYOFFS + k] = r;
         }
-        __syncthreads();
     }
 }
 
@@ -384,8 +426,10 @@ cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, c
 }
 
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
-                               TaskMoments *out) {
-    merge_tasks_kernel<<<n_tasks, 256, 0, s>>>(tasks, partials, out);
+                               TaskMoments *out, int64_t max_tiles) {
+    // one block per task; wide blocks only when some task has many tiles to read
+    const int threads = max_tiles >= 4096 ? 1024 : 256;
+    merge_tasks_kernel<<<n_tasks, threads, 0, s>>>(tasks, partials, out);
     return cudaGetLastError();
 }
 

@@ -208,3 +208,26 @@ def test_config0_plain_fp64_vs_closed_form(qk, handle, oracle):
     bias = abs(r["price"] - rf["price"])
     assert abs(r["price"] - exact) <= 3.0 * r["std_error"] + 2.0 * bias + 1e-3, (r, exact, rf)
     assert abs(rf["price"] - exact) <= 3.0 * rf["std_error"] + 1e-3
+
+
+def test_prepared_batch_graph_replay(qk, handle):
+    """The prepared set replays its captured launch sequence: every replay equals the one-shot
+    batched call bit for bit, uploads nothing, and another pricing call drops the prepared set."""
+    from quantkos_b200 import workloads as W
+    batch = W.mixed_batch(24, seed=5)
+    for c in batch:
+        c.n_paths = min(c.n_paths, 100_000)
+    g = W.batch_greeks()
+    want = qk.price_batch(batch, g, handle)
+    prep = qk.PreparedBatch(batch, g, handle)
+    for _ in range(2):
+        prep.run()
+        got = prep.fetch()
+        for a, b in zip(got, want):
+            assert a["legs"] == b["legs"]
+        t = handle.last_timing()
+        assert t["h2d_bytes"] == 0 and t["launches"] >= 2 and t["paths_ms"] > 0.0
+        assert t["device_ms"] >= t["paths_ms"]
+    qk.price_batch(batch[:1], None, handle)
+    with pytest.raises(RuntimeError, match="qk_batch_prepare"):
+        prep.run()
