@@ -58,6 +58,7 @@ def parse_args():
                     help="cpu_baseline leg of our arm: paths of the one timed sample (about 10-30 s of CPU work)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--paths", type=int, default=N_PATHS,
                     help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
     ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve"], default="bates5",
@@ -369,6 +370,13 @@ def main() -> None:
     contract = workload_contract(qk, rank, n_paths=args.paths)
     path_steps = float(args.paths) * N_STEPS
 
+    # ---- launch shape: the engine's autotuner on the workload itself (untimed)
+    tuned = None
+    if not args.no_autotune:
+        rep = h.autotune([contract], None, reps=1)[0]
+        tuned = {"tiles_per_warp": rep["tiles_per_warp"], "guided_tail": rep["guided_tail"],
+                 "best_ms": rep["best_ms"], "default_ms": rep["default_ms"]}
+
     # ---- value: descriptors resident in HBM, K device-timed pricings
     prep = qk.PreparedBatch([contract], None, h)
     for _ in range(max(args.warmup, 3)):
@@ -435,6 +443,48 @@ def main() -> None:
         except (ValueError, KeyError):
             traffic = None
 
+    # ---- the fused Heston-QE European kernel alone (same market, no jumps, one leg)
+    hqe = None
+    if not args.no_plain:
+        hc = qk.make_contract(S0=100.0, v0=0.04, r=0.03, q=0.0, model=qk.HESTON, scheme=qk.ANDERSEN_QE, kappa=2.0,
+                              theta=0.04, sigma=0.3, rho=-0.7, psi_c=1.5, T=1.0, n_steps=N_STEPS,
+                              n_paths=args.paths, seed=42, stream=rank, precision=qk.FP32,
+                              payoffs=[qk.payoff(qk.EUROPEAN, qk.CALL, 100.0)])
+        hp = qk.PreparedBatch([hc], None, h)
+        hms = []
+        for i in range(3 + 5):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            hp.run()
+            hp.fetch()
+            if i >= 3:
+                hms.append(h.last_timing()["paths_ms"])
+        h_ps = path_steps / (statistics.mean(hms) * 1e-3)
+        hqe = {"workload": f"heston_qe_european_call_{args.paths}x{N_STEPS}_fp32", "kernel_ms": statistics.mean(hms),
+               "achieved": h_ps / 1e9, "peak": sfu_ops / SFU_PER_STEP / 1e9, "unit": "Gpath-steps/s",
+               "frac": h_ps / (sfu_ops / SFU_PER_STEP)}
+
+    # ---- the same workload with antithetic pairs: throughput and standard error per leg
+    anti = None
+    if not args.no_plain:
+        ac = workload_contract(qk, rank, n_paths=args.paths)
+        ac.antithetic = 1
+        ap = qk.PreparedBatch([ac], None, h)
+        ams, r_anti = [], None
+        for i in range(3 + 5):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            ap.run()
+            r_anti = ap.fetch()
+            if i >= 3:
+                ams.append(h.last_timing()["device_ms"])
+        a_ms = statistics.mean(ams)
+        ratio = [ra["std_error"] / rp["std_error"] for ra, rp in zip(r_anti[0]["legs"], res[0]["legs"])]
+        anti = {"ms": a_ms, "value": path_steps / (a_ms * 1e-3), "unit": METRIC,
+                "se_ratio_vs_independent": ratio,
+                "equal_se_speedup": [ms_per_step / (a_ms * q * q) for q in ratio],
+                "price": [leg["price"] for leg in r_anti[0]["legs"]]}
+
     # ---- plain FP64 drop-in on the same workload (equal paths => equal standard error)
     plain = None
     if not args.no_plain:
@@ -479,6 +529,9 @@ def main() -> None:
                          "peak_source": f"measured SFU rate {sfu_ops / 1e12:.3f} Tops/s (qk_measure_sfu); "
                                         f"{SFU_PER_STEP:.0f} SFU ops per path-step (algorithmic)"},
             "cpu_baseline": cpu,
+            "heston_qe_european": hqe,
+            "antithetic": anti,
+            "autotune": tuned,
             "plain_fp64": plain,
             "clocks": clocks,
             "gpu_launches": launches,

@@ -147,6 +147,7 @@ typedef struct {
     uint32_t w_first; /* word of the step's first Poisson uniform */
     uint32_t wx[4];
     int domain;
+    int neg; /* antithetic member: the jump normal is negated */
 } Draws;
 
 static double draw_uniform_d(Draws *d, int as_float) {
@@ -226,7 +227,7 @@ static void step_d(const Inv *p, int model, int scheme, double *S_io, double *v_
         if (N > 0) {
             double Z;
             if (d->fed) Z = d->z[2];
-            else { uint32_t w[4]; double z2; philox_block(d->step, d->path, d->stream, 1u, d->k0, d->k1, w); bm_d(w[0], w[1], &Z, &z2); }
+            else { uint32_t w[4]; double z2; philox_block(d->step, d->path, d->stream, 1u, d->k0, d->k1, w); bm_d(w[0], w[1], &Z, &z2); if (d->neg) Z = -Z; }
             Sn *= exp((double)N * p->mu_j + sqrt((double)N) * p->sigma_j * Z);
         }
     }
@@ -302,7 +303,7 @@ static void step_f(const InvF *p, int model, int scheme, float *S_io, float *v_i
         if (N > 0) {
             float Z;
             if (d->fed) Z = (float)d->z[2];
-            else { uint32_t w[4]; float z2; philox_block(d->step, d->path, d->stream, 1u, d->k0, d->k1, w); bm_f(w[0], w[1], &Z, &z2); }
+            else { uint32_t w[4]; float z2; philox_block(d->step, d->path, d->stream, 1u, d->k0, d->k1, w); bm_f(w[0], w[1], &Z, &z2); if (d->neg) Z = -Z; }
             Sn *= expf((float)N * p->mu_j + sqrtf((float)N) * p->sigma_j * Z);
         }
     }
@@ -359,8 +360,9 @@ static void normalise(const qk_contract *c, qk_contract *n, double *scale) {
 }
 
 /* store: optional callback rows (every `stride` steps) into S_rows/v_rows[row*ld + col] */
-static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_t path, PathOut *o, int stride,
-                     double *S_rows, double *v_rows, int64_t ld, int64_t col) {
+/* neg: the antithetic member of pair `path` (every normal negated, uniforms shared) */
+static void run_path_sign(const qk_contract *c, const Inv *p, const InvF *pf, uint32_t path, int neg, PathOut *o,
+                          int stride, double *S_rows, double *v_rows, int64_t ld, int64_t col) {
     const uint32_t k0 = (uint32_t)(c->seed & 0xFFFFFFFFu), k1 = (uint32_t)(c->seed >> 32);
     const uint32_t stream = (uint32_t)c->stream;
     const int fp32 = c->precision == QK_FP32;
@@ -373,6 +375,7 @@ static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_
         Draws d;
         memset(&d, 0, sizeof(d));
         d.k0 = k0; d.k1 = k1; d.path = path; d.stream = stream; d.step = (uint32_t)n;
+        d.neg = neg;
         /* normal pair of step n: domain 0, block n/2, words (x,y) for even n, (z,w) for odd n */
         if ((n & 1) == 0) philox_block((uint32_t)(n >> 1), path, stream, 0u, k0, k1, w);
         const uint32_t wa = (n & 1) ? w[2] : w[0];
@@ -384,6 +387,7 @@ static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_
         if (fp32) {
             float z1, z2;
             bm_f(wa, wb, &z1, &z2);
+            if (neg) { z1 = -z1; z2 = -z2; }
             step_f(pf, c->model, c->scheme, &Sf, &vf, z1, z2, &d);
             ssum += (double)Sf;
             smaxf = fmaxf(smaxf, Sf);
@@ -392,6 +396,7 @@ static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_
         } else {
             double z1, z2;
             bm_d(wa, wb, &z1, &z2);
+            if (neg) { z1 = -z1; z2 = -z2; }
             step_d(p, c->model, c->scheme, &S, &v, z1, z2, &d);
             ssum += S;
             smax = fmax(smax, S);
@@ -408,6 +413,11 @@ static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_
     o->ssum = ssum;
     o->smax = fp32 ? (double)smaxf : smax;
     o->smin = fp32 ? (double)sminf : smin;
+}
+
+static void run_path(const qk_contract *c, const Inv *p, const InvF *pf, uint32_t path, PathOut *o, int stride,
+                     double *S_rows, double *v_rows, int64_t ld, int64_t col) {
+    run_path_sign(c, p, pf, path, 0, o, stride, S_rows, v_rows, ld, col);
 }
 
 /* Payoff.hpp:51-72, 157-242, in double (float legs rounded through float like the FP32 build). */
@@ -512,14 +522,30 @@ static void forward_moments(const qk_contract *n, Mom *legs) {
 #endif
         Mom loc[QK_MAX_PAYOFFS];
         memset(loc, 0, sizeof(loc));
+        if (n->antithetic) {
+            /* one sample per antithetic pair: the average of its two payoffs */
 #pragma omp for schedule(static)
-        for (int64_t i = 0; i < n->n_paths; ++i) {
-            PathOut o;
-            run_path(n, &p, &pf, (uint32_t)i, &o, 0, NULL, NULL, 0, 0);
-            for (int k = 0; k < nl; ++k) {
-                const double x = payoff_of(&n->payoffs[k], &o, n->n_steps, fp32);
-                Mom one = {1.0, x, 0.0, x > eps ? 1.0 : 0.0};
-                loc[k] = mom_merge(loc[k], one);
+            for (int64_t i = 0; i < n->n_paths / 2; ++i) {
+                PathOut oa, ob;
+                run_path_sign(n, &p, &pf, (uint32_t)i, 0, &oa, 0, NULL, NULL, 0, 0);
+                run_path_sign(n, &p, &pf, (uint32_t)i, 1, &ob, 0, NULL, NULL, 0, 0);
+                for (int k = 0; k < nl; ++k) {
+                    const double xa = payoff_of(&n->payoffs[k], &oa, n->n_steps, fp32);
+                    const double xb = payoff_of(&n->payoffs[k], &ob, n->n_steps, fp32);
+                    Mom one = {1.0, 0.5 * (xa + xb), 0.0, 0.5 * ((xa > eps ? 1.0 : 0.0) + (xb > eps ? 1.0 : 0.0))};
+                    loc[k] = mom_merge(loc[k], one);
+                }
+            }
+        } else {
+#pragma omp for schedule(static)
+            for (int64_t i = 0; i < n->n_paths; ++i) {
+                PathOut o;
+                run_path(n, &p, &pf, (uint32_t)i, &o, 0, NULL, NULL, 0, 0);
+                for (int k = 0; k < nl; ++k) {
+                    const double x = payoff_of(&n->payoffs[k], &o, n->n_steps, fp32);
+                    Mom one = {1.0, x, 0.0, x > eps ? 1.0 : 0.0};
+                    loc[k] = mom_merge(loc[k], one);
+                }
             }
         }
         for (int k = 0; k < nl; ++k) part[(size_t)tid * QK_MAX_PAYOFFS + k] = loc[k];

@@ -32,6 +32,7 @@ class Contract(C.Structure):
         ("precision", C.c_int32), ("n_payoffs", C.c_int32),
         ("payoffs", Payoff * QK_MAX_PAYOFFS),
         ("lsm_basis", C.c_int32), ("lsm_dates", C.c_int32),
+        ("antithetic", C.c_int32), ("reserved_", C.c_int32),
     ]
 
 

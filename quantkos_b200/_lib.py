@@ -53,6 +53,7 @@ class Contract(C.Structure):
         ("precision", C.c_int32), ("n_payoffs", C.c_int32),
         ("payoffs", Payoff * QK_MAX_PAYOFFS),
         ("lsm_basis", C.c_int32), ("lsm_dates", C.c_int32),
+        ("antithetic", C.c_int32), ("reserved_", C.c_int32),
     ]
 
 
@@ -75,6 +76,16 @@ class Timing(C.Structure):
     _fields_ = [("device_ms", C.c_double), ("paths_ms", C.c_double), ("reduce_ms", C.c_double),
                 ("launches", C.c_int64), ("path_steps", C.c_double), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64)]
+
+
+TUNE_KINDS = 12
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_kinds", C.c_int32), ("precision", C.c_int32 * TUNE_KINDS), ("model", C.c_int32 * TUNE_KINDS),
+                ("scheme", C.c_int32 * TUNE_KINDS), ("tiles_per_warp", C.c_int32 * TUNE_KINDS),
+                ("guided_tail", C.c_int32 * TUNE_KINDS), ("best_ms", C.c_double * TUNE_KINDS),
+                ("default_ms", C.c_double * TUNE_KINDS), ("candidates", C.c_int32)]
 
 
 class ServeStats(C.Structure):
@@ -116,6 +127,8 @@ SIGNATURES = {
     "qk_destroy": (C.c_int, [_VP]),
     "qk_get_stream": (C.c_int, [_VP, _P(_VP)]),
     "qk_last_timing": (C.c_int, [_VP, _P(Timing)]),
+    "qk_autotune": (C.c_int, [_VP, _P(Contract), C.c_int32, _P(Greeks), C.c_int32, _P(TuneReport)]),
+    "qk_tune_set": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "qk_measure_sfu": (C.c_int, [_VP, _P(C.c_double)]),
     "qk_validate": (C.c_int, [_P(Contract), _P(Greeks)]),
     "qk_price_plain": (C.c_int, [_VP, _P(Contract), _P(Greeks), _P(Result)]),

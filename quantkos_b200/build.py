@@ -34,7 +34,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
-SOURCES = ["qk_paths.cu", "qk_lsm.cu", "qk_api.cu", "qk_serve.cu", "qk_config.cu", "qk_noalloc.cu"]
+SOURCES = ["qk_paths.cu", "qk_lsm.cu", "qk_api.cu", "qk_serve.cu", "qk_config.cu", "qk_tune.cu", "qk_noalloc.cu"]
 
 
 def _run(cmd: list[str], cwd: Path | None = None) -> None:
@@ -74,7 +74,7 @@ def build_engine(force: bool = False) -> Path:
 
 def build_oracle(force: bool = False) -> Path:
     src = ORACLE_DIR / "qk_oracle.c"
-    if force or _stale(ORACLE_LIB, [src]):
+    if force or _stale(ORACLE_LIB, [src, ROOT / "include" / "quantkos_b200.h"]):
         _run(["gcc", "-std=c11", "-O2", "-fPIC", "-shared", "-fopenmp", "-o", str(ORACLE_LIB), str(src), "-lm"])
     return ORACLE_LIB
 

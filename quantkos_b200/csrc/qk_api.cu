@@ -22,9 +22,7 @@
 
 namespace qk {
 
-namespace {
 thread_local std::string g_last_error;
-}
 
 void set_error(const std::string &msg) { g_last_error = msg; }
 qk_status fail(qk_status s, const std::string &msg) {
@@ -91,6 +89,11 @@ qk_status validate_contract(const qk_contract &c, const qk_greeks *g) {
             return fail(QK_ERR_INVALID_ARG, "Config Error: Strike price (K) is absurdly high (exceeds 10000x of S0). This will likely result in zero-variance path generation and statistical breakdown.");
         if (p.type == QK_AMERICAN) american = true;
     }
+    if (c.antithetic != 0 && c.antithetic != 1) return fail(QK_ERR_INVALID_ARG, "antithetic must be 0 or 1");
+    if (c.antithetic && (c.n_paths % 2) != 0)
+        return fail(QK_ERR_INVALID_ARG, field("MC", "N_Paths", "must be even for antithetic sampling."));
+    if (c.antithetic && american)
+        return fail(QK_ERR_UNSUPPORTED, "antithetic sampling covers forward payoff legs only (not American)");
     if (american) {
         if (c.n_payoffs != 1) return fail(QK_ERR_INVALID_ARG, "an American contract carries exactly one payoff leg");
         if (c.lsm_basis != QK_LSM_LAGUERRE3 && c.lsm_basis != QK_LSM_POLY_SV) return fail(QK_ERR_INVALID_ARG, "lsm_basis invalid");
@@ -214,8 +217,12 @@ TaskDev make_task(const qk_contract &b, int ppt) {
     const float Lf = t.cf.exp_m_lambda_dt;
     const double kd = std::ceil(static_cast<double>(Lf) * 8388608.0 - 0.5);
     t.jump_kmin = static_cast<uint32_t>(std::min(std::max(kd, 0.0), 8388608.0));
-    const int64_t tile_paths = static_cast<int64_t>(kWarpTilePaths) * ppt;
-    t.n_tiles = static_cast<int32_t>((b.n_paths + tile_paths - 1) / tile_paths);
+    t.antithetic = b.antithetic ? 1 : 0;
+    const int64_t units = t.antithetic ? b.n_paths / 2 : b.n_paths;  // a lane simulates a path or a pair
+    const int64_t tile_units = static_cast<int64_t>(kWarpTilePaths) * ppt;
+    t.n_tiles = static_cast<int32_t>((units + tile_units - 1) / tile_units);
+    t.n_big = t.n_tiles;  // uniform tiles unless split_tail is applied
+    t.ppt_tail = ppt;
     for (int k = 0; k < b.n_payoffs; ++k) {
         t.pay[k].type = b.payoffs[k].type;
         t.pay[k].right = b.payoffs[k].right;
@@ -225,19 +232,43 @@ TaskDev make_task(const qk_contract &b, int ppt) {
     return t;
 }
 
+// Guided tail for a task that fills the GPU many times over on its own: big tiles
+// of 2 x ppt rounds first, then the last rounds (about half a big tile per warp
+// slot) in tiles of a quarter of ppt.  Warps that finish their last big tile early
+// take short tail tiles, so all warps end within a short tile of each other; the
+// record count stays below that of uniform ppt-round tiles.
+static void split_tail(TaskDev &t, int64_t warp_slots) {
+    const int64_t units = t.antithetic ? t.n_paths / 2 : t.n_paths;
+    const int64_t rounds = (units + kWarpTilePaths - 1) / kWarpTilePaths;
+    if (t.ppt < 4 || rounds < 4 * warp_slots * static_cast<int64_t>(t.ppt)) return;
+    const int big = 2 * t.ppt;
+    const int tail = std::max(1, t.ppt / 4);
+    const int64_t tail_target = warp_slots * big / 2;
+    const int64_t n_big = (rounds - tail_target) / big;
+    const int64_t tail_rounds = rounds - n_big * big;
+    t.ppt = big;
+    t.ppt_tail = tail;
+    t.n_big = static_cast<int32_t>(n_big);
+    t.n_tiles = static_cast<int32_t>(n_big + (tail_rounds + tail - 1) / tail);
+}
+
 // Relative device cost of one path-step (QE and jumps cost more SFU work).
 static double step_cost(const TaskDev &t) {
     double c = 1.0;
     if (t.scheme == QK_ANDERSEN_QE) c *= 1.6;
     if (t.model == QK_BATES) c *= 1.25;
     if (t.precision == QK_FP64) c *= 6.0;
+    if (t.antithetic) c *= 1.7;  // two paths per lane, one set of draws
     return c;
 }
 
+// The plain method's launch shape (one task per launch; not tuned).
+constexpr int kPlainTilesPerWarp = 24;
+
 // Rounds per warp tile: enough tiles to keep every warp slot of the GPU busy
 // several times over, few enough that per-tile records stay negligible.
-int choose_ppt(int64_t n_paths, int64_t total_paths_all, int sm_count) {
-    const int64_t target_tiles = static_cast<int64_t>(sm_count) * 32 * 12;
+int choose_ppt(int64_t n_paths, int64_t total_paths_all, int sm_count, int tiles_per_warp) {
+    const int64_t target_tiles = static_cast<int64_t>(sm_count) * 32 * tiles_per_warp;
     int64_t ppt = total_paths_all / (target_tiles * kWarpTilePaths);
     ppt = std::max<int64_t>(1, std::min<int64_t>(ppt, 64));
     const int64_t need = (n_paths + kWarpTilePaths - 1) / kWarpTilePaths;
@@ -293,7 +324,8 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     plan.norm.resize(n);
     plan.status.assign(n, QK_OK);
     plan.task_of.assign(static_cast<size_t>(n) * kNumRoles, -1);
-    int64_t total_paths = 0;
+    // paths per kernel kind (precision, model, scheme): each kind is one launch
+    int64_t kind_paths[2][2][3][2] = {};  // [precision][model][scheme][antithetic]: lanes' units per launch
     for (int i = 0; i < n; ++i) {
         const qk_greeks *g = plan.g_of(i);
         const qk_status s = validate_contract(cs[i], g);
@@ -304,7 +336,10 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
             plan.american.push_back(i);
             continue;
         }
-        total_paths += cs[i].n_paths * static_cast<int64_t>(roles_for(g, cs[i].T).size());
+        const int pr = plain ? QK_FP64 : cs[i].precision;
+        const int64_t units = cs[i].antithetic ? cs[i].n_paths / 2 : cs[i].n_paths;
+        kind_paths[pr][cs[i].model][cs[i].scheme][cs[i].antithetic ? 1 : 0] +=
+            units * static_cast<int64_t>(roles_for(g, cs[i].T).size());
     }
     struct Item {
         TaskDev t;
@@ -314,12 +349,21 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     std::vector<Item> items;
     for (int i = 0; i < n; ++i) {
         if (cs[i].payoffs[0].type == QK_AMERICAN) continue;
-        const int ppt = plain ? choose_ppt(cs[i].n_paths, cs[i].n_paths, h->sm_count)
-                              : choose_ppt(cs[i].n_paths, total_paths, h->sm_count);
+        const int pr = plain ? QK_FP64 : cs[i].precision;
+        const bool anti = cs[i].antithetic != 0;
+        const int64_t units = anti ? cs[i].n_paths / 2 : cs[i].n_paths;
+        const int64_t launch_units = plain ? units : kind_paths[pr][cs[i].model][cs[i].scheme][anti ? 1 : 0];
+        const int ppt = choose_ppt(units, launch_units, h->sm_count,
+                                   plain ? kPlainTilesPerWarp : h->tune_tpw[pr][cs[i].model][cs[i].scheme]);
+        const bool tail = !plain && h->tune_tail[pr][cs[i].model][cs[i].scheme];
+        const int64_t warp_slots = static_cast<int64_t>(h->sm_count) *
+                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, anti) *
+                                   (kPathBlock / 32);
         const qk_greeks *g = plan.g_of(i);
         for (int role : roles_for(g, cs[i].T)) {
             const qk_contract b = bumped(plan.norm[i], g, role);
             Item it{make_task(b, ppt), i, role, 0.0};
+            if (tail) split_tail(it.t, warp_slots);
             it.cost = step_cost(it.t) * b.n_steps * b.n_payoffs * 0.02 + step_cost(it.t) * b.n_steps;
             items.push_back(it);
         }
@@ -328,18 +372,22 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         // group by kernel (precision, model, scheme); longest tiles first inside a group
         std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
             if (a.t.precision != b.t.precision) return a.t.precision < b.t.precision;
+            if (a.t.antithetic != b.t.antithetic) return a.t.antithetic < b.t.antithetic;
             if (a.t.model != b.t.model) return a.t.model < b.t.model;
             if (a.t.scheme != b.t.scheme) return a.t.scheme < b.t.scheme;
             return a.cost > b.cost;
         });
     }
-    int64_t slot = 0, rec = 0;
+    int64_t slot = 0, rec = 0, chunk = 0;
     for (size_t k = 0; k < items.size(); ++k) {
         TaskDev &t = items[k].t;
         t.tile_begin = slot;
         t.partial_base = rec;
+        t.chunk_base = chunk;
+        t.n_chunks = (t.n_tiles + kMergeChunkTiles - 1) / kMergeChunkTiles;
         slot += t.n_tiles;
         rec += static_cast<int64_t>(t.n_tiles) * t.n_payoffs;
+        chunk += t.n_chunks;
         plan.tasks.push_back(t);
         plan.task_contract.push_back(items[k].contract);
         plan.task_role.push_back(items[k].role);
@@ -348,6 +396,7 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     }
     plan.total_slots = slot;
     plan.total_records = rec;
+    plan.total_chunks = chunk;
     plan.plain = plain;
     return QK_OK;
 }
@@ -361,6 +410,8 @@ static qk_status upload_plan(qk_handle *h, const Plan &plan) {
     if ((s = h->d_prefix.ensure(nt * sizeof(int64_t))) != QK_OK) return s;
     if ((s = h->d_partials.ensure(static_cast<size_t>(plan.total_records) * sizeof(Moments))) != QK_OK) return s;
     if ((s = h->d_moments.ensure(nt * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK) return s;
+    if ((s = h->d_chunks.ensure(static_cast<size_t>(plan.total_chunks) * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK)
+        return s;
     if ((s = h->d_cursor.ensure(nt * sizeof(unsigned long long))) != QK_OK) return s;
     if ((s = h->h_tasks.ensure(nt * sizeof(TaskDev) + nt * sizeof(int64_t))) != QK_OK) return s;
     if ((s = h->h_moments.ensure(nt * QK_MAX_PAYOFFS * sizeof(Moments))) != QK_OK) return s;
@@ -390,12 +441,13 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
     if (plan.plain) {
         for (size_t i = 0; i < nt; ++i) {
             const TaskDev &t = plan.tasks[i];
-            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme);
+            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme, t.antithetic != 0);
             const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
             // one task: its own queue cursor, its own tile range (prefix of one task = itself)
             const uint64_t seed = static_cast<uint64_t>(t.key0) | (static_cast<uint64_t>(t.key1) << 32);
             QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
-                                           t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed));
+                                           t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed,
+                                           t.antithetic != 0));
             h->launches++;
         }
     } else {
@@ -404,11 +456,11 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             size_t e = b;
             const TaskDev &tb = plan.tasks[b];
             while (e < nt && plan.tasks[e].precision == tb.precision && plan.tasks[e].model == tb.model &&
-                   plan.tasks[e].scheme == tb.scheme)
+                   plan.tasks[e].scheme == tb.scheme && plan.tasks[e].antithetic == tb.antithetic)
                 ++e;
             const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
             const int64_t slots = slots_end - tb.tile_begin;
-            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme);
+            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.antithetic != 0);
             const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
             bool uniform_key = true;
             for (size_t i = b; i < e; ++i)
@@ -416,17 +468,16 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
             QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
                                            static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
-                                           uniform_key, seed));
+                                           uniform_key, seed, tb.antithetic != 0));
             h->launches++;
             b = e;
         }
     }
     QK_CUDA_TRY(cudaEventRecordWithFlags(h->ev_paths1, h->stream, ev_flags));
-    int64_t max_tiles = 0;
-    for (const TaskDev &t : plan.tasks) max_tiles = std::max<int64_t>(max_tiles, t.n_tiles);
-    QK_CUDA_TRY(launch_merge_tasks(static_cast<int>(nt), h->stream, dt, dpart,
-                                   static_cast<Moments *>(h->d_moments.ptr), max_tiles));
-    h->launches++;
+    QK_CUDA_TRY(launch_merge_two_level(static_cast<int>(nt), plan.total_chunks, h->stream, dt, dpart,
+                                       static_cast<Moments *>(h->d_chunks.ptr),
+                                       static_cast<Moments *>(h->d_moments.ptr)));
+    h->launches += 2;
     QK_CUDA_TRY(cudaMemcpyAsync(h->h_moments.ptr, h->d_moments.ptr, nt * QK_MAX_PAYOFFS * sizeof(Moments),
                                 cudaMemcpyDeviceToHost, h->stream));
     return QK_OK;
@@ -563,6 +614,7 @@ qk_status assemble_results(qk_handle *h, const Plan &plan, const Moments *task_m
 qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &out) {
     qk_status s = validate_contract(c, nullptr);
     if (s != QK_OK) return s;
+    if (c.antithetic) return fail(QK_ERR_UNSUPPORTED, "per-path payoffs of antithetic pairs are not dumped");
     QK_CUDA_TRY(cudaSetDevice(h->device));
     double scale = 1.0;
     const qk_contract n = normalised(c, &scale);
@@ -670,6 +722,7 @@ qk_status qk_destroy(qk_handle *h) {
     h->d_prefix.release();
     h->d_partials.release();
     h->d_moments.release();
+    h->d_chunks.release();
     h->d_cursor.release();
     h->d_trace.release();
     h->h_tasks.release();
@@ -823,6 +876,7 @@ qk_status qk_paths_dump(qk_handle *h, const qk_contract *c, int64_t first, int64
     if (!h || !c || !S_out || count < 1 || first < 0) return fail(QK_ERR_INVALID_ARG, "invalid dump arguments");
     qk_status s = validate_contract(*c, nullptr);
     if (s != QK_OK) return s;
+    if (c->antithetic) return fail(QK_ERR_UNSUPPORTED, "qk_paths_dump: antithetic pairs are not dumped");
     if (first + count > c->n_paths) return fail(QK_ERR_INVALID_ARG, "path range beyond n_paths");
     QK_CUDA_TRY(cudaSetDevice(h->device));
     double scale = 1.0;

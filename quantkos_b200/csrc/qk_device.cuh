@@ -334,6 +334,23 @@ __device__ __noinline__ R jump_factor(const StepConst<R> &p, R prod, Draws &d) {
     return Math<R>::exp(rN * p.mu_j + Math<R>::sqrt(rN) * p.sigma_j * Z);
 }
 
+// Both members of an antithetic pair: the same jump count, jump sizes with the
+// normal of opposite sign.
+template <class R, class Draws>
+__device__ __noinline__ void jump_factor_pair(const StepConst<R> &p, R prod, Draws &d, R &fa, R &fb) {
+    int N = 0;
+    do {
+        ++N;
+        prod *= d.uniform();
+    } while (prod >= p.exp_m_lambda_dt && N < kMaxJumpsPerStep);
+    const R Z = d.jump_normal();
+    const R rN = static_cast<R>(N);
+    const R m = rN * p.mu_j;
+    const R s = Math<R>::sqrt(rN) * p.sigma_j * Z;
+    fa = Math<R>::exp(m + s);
+    fb = Math<R>::exp(m - s);
+}
+
 template <class R, class Draws>
 __device__ __forceinline__ void bates_jump(const StepConst<R> &p, R &S, Draws &d) {
     const R first = d.uniform();
@@ -424,6 +441,20 @@ __device__ __forceinline__ Moments warp_moments(double x, bool active, bool itm)
     const double dv = active ? x - mean : 0.0;
     const double m2 = warp_sum(dv * dv);
     return Moments{n, mean, m2, static_cast<double>(__popc(im))};
+}
+
+// Moments of the 32 pair averages of a warp (antithetic sampling): each lane's
+// value is (x_a + x_b) / 2 and its in-the-money weight (1{a} + 1{b}) / 2.
+__device__ __forceinline__ Moments warp_moments_pair(double y, bool active, bool itm_a, bool itm_b) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    const unsigned ia = __ballot_sync(0xffffffffu, active && itm_a);
+    const unsigned ib = __ballot_sync(0xffffffffu, active && itm_b);
+    const double n = static_cast<double>(__popc(act));
+    const double s = warp_sum(active ? y : 0.0);
+    const double mean = n > 0.0 ? s / n : 0.0;
+    const double dv = active ? y - mean : 0.0;
+    const double m2 = warp_sum(dv * dv);
+    return Moments{n, mean, m2, 0.5 * static_cast<double>(__popc(ia) + __popc(ib))};
 }
 
 }  // namespace qk

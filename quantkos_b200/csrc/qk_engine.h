@@ -47,6 +47,7 @@ struct Plan {
     std::vector<int> american;         // contracts priced by LSM
     int64_t total_slots = 0;
     int64_t total_records = 0;
+    int64_t total_chunks = 0;  // level-1 merge chunks over all tasks
     double path_steps = 0.0;
     double lsm_path_steps = 0.0;
     std::vector<LsmTaskInfo> lsm_tasks;
@@ -64,7 +65,7 @@ struct qk_handle {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_paths0 = nullptr, ev_paths1 = nullptr, ev_end = nullptr;
-    qk::DevArena d_tasks, d_prefix, d_partials, d_moments, d_cursor, d_trace;
+    qk::DevArena d_tasks, d_prefix, d_partials, d_moments, d_cursor, d_trace, d_chunks;
     qk::HostArena h_tasks, h_moments, h_lsm;
     qk::DevArena d_lsm_moments;
     qk::LsmArena lsm;
@@ -72,6 +73,9 @@ struct qk_handle {
     bool prepared = false;
     cudaGraphExec_t graph = nullptr;  // the prepared batch's launch sequence (qk_batch_prepare)
     int64_t graph_launches = 0;
+    // launch shape per kernel kind [precision][model][scheme] (autotuner)
+    int tune_tpw[2][2][3] = {{{24, 24, 24}, {24, 24, 24}}, {{24, 24, 24}, {24, 24, 24}}};
+    int tune_tail[2][2][3] = {};
     qk_timing timing{};
     int64_t launches = 0;
     int64_t h2d_bytes = 0, d2h_bytes = 0;

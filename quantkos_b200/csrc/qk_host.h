@@ -13,6 +13,7 @@ namespace qk {
 // Thread-local message behind qk_last_error().
 void set_error(const std::string &msg);
 qk_status fail(qk_status s, const std::string &msg);
+extern thread_local std::string g_last_error;  // message of the last failing call on this thread
 
 // UInputs::validate (include/core/config/Config.hpp:63-84, 119-137, 198-305, 347-373,
 // 442-563) on the fields a contract carries, plus this engine's own limits.

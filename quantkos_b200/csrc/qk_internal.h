@@ -71,7 +71,12 @@ struct TaskDev {
     int64_t tile_begin;    // first queue slot of the task (tiles of a task are consecutive)
     int64_t partial_base;  // first per-tile moments record of the task
     int32_t n_tiles;
-    int32_t ppt;           // paths per thread per tile: a tile is kPathBlock * ppt paths
+    int32_t ppt;           // rounds of a big tile: a round is one path per lane of a warp
+    int32_t n_big;         // tiles 0 .. n_big-1 have ppt rounds; the rest (the tail) ppt_tail rounds
+    int32_t ppt_tail;
+    int64_t chunk_base;    // first merge chunk of the task (two-level merge of the tile records)
+    int32_t n_chunks;      // merge chunks of the task: ceil(n_tiles / kMergeChunkTiles)
+    int32_t antithetic;    // 1: a lane simulates pair u (paths 2u, 2u+1); tiles count pairs
     PayoffSpec pay[QK_MAX_PAYOFFS];
 };
 

@@ -16,18 +16,27 @@ constexpr int kPathMinBlocksFp32 = QK_PATH_MIN_BLOCKS_FP32;  // resident blocks 
 
 // uniform_key: every task of the launch has Philox key `seed` (round keys go in the
 // kernel parameters); otherwise each task's key is read from its descriptor.
+// antithetic: every task of the launch samples antithetic pairs.
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
-                               unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed);
+                               unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
+                               bool antithetic = false);
 // max_tiles: the largest n_tiles among the tasks (sets the block width).
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
                                TaskMoments *out, int64_t max_tiles = 0);
+// Tile records per level-1 merge chunk.
+constexpr int kMergeChunkTiles = 512;
+// Two-level merge: level 1 reduces chunks of kMergeChunkTiles tile records
+// (n_chunks = sum of the tasks' n_chunks) into chunks[n_chunks][QK_MAX_PAYOFFS],
+// level 2 reduces each task's chunk records into out[task][QK_MAX_PAYOFFS].
+cudaError_t launch_merge_two_level(int n_tasks, int64_t n_chunks, cudaStream_t s, const TaskDev *tasks,
+                                   const Moments *partials, Moments *chunks, TaskMoments *out);
 cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t seed, cudaStream_t s, const TaskDev *task,
                               int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld);
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
                               int umax, int n, double *S_out, double *v_out, int *status);
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme);
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, bool antithetic = false);
 // Times a kernel of independent ex2.approx chains; returns its duration and MUFU op count.
 cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
                              double *ops);

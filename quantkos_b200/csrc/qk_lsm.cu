@@ -10,9 +10,10 @@
 // Here: the forward kernel writes spot (and variance) only at the exercise
 // dates, as SoA slabs slab[date][path] in HBM; the backward sweep is one kernel
 // per date that applies the exercise decision of date d and accumulates the
-// regression sums of date d-1 in the same pass; a one-block kernel reduces the
-// block sums and solves the normal equations in FP64 on the device.  No host
-// round trip happens inside the sweep.
+// regression sums of date d-1 in the same pass, streaming the slabs through
+// shared memory with cp.async; the last block to finish reduces the block sums
+// and solves the normal equations in FP64 on the device.  No host round trip
+// happens inside the sweep.
 //
 // Two regression modes:
 //   QK_LSM_LAGUERRE3 — the reference's: X = S/K, Laguerre L0..L3 (LSMAmerican.hpp:157-199),
@@ -37,6 +38,9 @@
 namespace qk {
 
 constexpr int kLsmBlock = 256;
+#ifndef QK_LSM_MIN_BLOCKS
+#define QK_LSM_MIN_BLOCKS 2  // resident sweep blocks per SM the register budget is set for
+#endif
 constexpr int kMaxCoef = 8;
 
 template <int BASIS>
@@ -67,38 +71,121 @@ __device__ __forceinline__ R lsm_intrinsic(int right, R S, R K) {
     return right == kCall ? (S > K ? S - K : R(0)) : (K > S ? K - S : R(0));
 }
 
-// Basis values of one path at one date.
-template <class R, int BASIS>
-__device__ __forceinline__ void eval_basis(R S, R v, R K, double cx, double cv, R *b) {
-    if constexpr (BASIS == QK_LSM_LAGUERRE3) {
-        // LaguerreBasis<4>::evaluate, Horner form (LSMAmerican.hpp:183-192)
-        const R X = S / K;
-        b[0] = R(1);
-        b[1] = R(1) - X;
-        b[2] = ((R(0.5) * X - R(2)) * X) + R(1);
-        b[3] = (((static_cast<R>(-1.0 / 6.0) * X + R(1.5)) * X - R(3)) * X) + R(1);
-    } else {
-        const R x = S / K - static_cast<R>(cx);
-        const R w = v - static_cast<R>(cv);
-        b[0] = R(1);
-        b[1] = x;
-        b[2] = x * x;
-        b[3] = x * x * x;
-        b[4] = w;
-        b[5] = x * w;
-    }
+// Basis values of one path at one date.  LAGUERRE3 in the working precision
+// (LaguerreBasis<4>::evaluate, Horner form, LSMAmerican.hpp:183-192); POLY_SV in
+// double on the centred coordinates x = S/K - c_x, w = v - c_v.
+template <class R>
+__device__ __forceinline__ void laguerre_basis(R S, R K, R *b) {
+    const R X = S / K;
+    b[0] = R(1);
+    b[1] = R(1) - X;
+    b[2] = ((R(0.5) * X - R(2)) * X) + R(1);
+    b[3] = (((static_cast<R>(-1.0 / 6.0) * X + R(1.5)) * X - R(3)) * X) + R(1);
+}
+
+struct PolyPoint {
+    double x, w;
+};
+template <class R>
+__device__ __forceinline__ PolyPoint poly_point(R S, R v, double inv_K, double cx, double cv) {
+    return PolyPoint{static_cast<double>(S) * inv_K - cx, static_cast<double>(v) - cv};
 }
 
 // Expected value of holding: sum of coefficients times basis, in double (LSMAmerican.hpp:484-502).
 template <class R, int BASIS>
-__device__ __forceinline__ double continuation(const double *c, R S, R v, R K, double cx, double cv) {
-    constexpr int NB = BasisTraits<BASIS>::NB;
-    R b[NB];
-    eval_basis<R, BASIS>(S, v, K, cx, cv, b);
-    double s = 0.0;
+__device__ __forceinline__ double continuation(const double *c, R S, R v, R K, double inv_K, double cx, double cv) {
+    if constexpr (BASIS == QK_LSM_LAGUERRE3) {
+        R b[4];
+        laguerre_basis<R>(S, K, b);
+        double s = 0.0;
 #pragma unroll
-    for (int i = 0; i < NB; ++i) s += c[i] * static_cast<double>(b[i]);
-    return s;
+        for (int i = 0; i < 4; ++i) s += c[i] * static_cast<double>(b[i]);
+        return s;
+    } else {
+        const PolyPoint q = poly_point<R>(S, v, inv_K, cx, cv);
+        const double x = q.x, w = q.w;
+        return c[0] + x * (c[1] + x * (c[2] + x * c[3])) + w * (c[4] + x * c[5]);
+    }
+}
+
+// Regression sums kept per thread.  LAGUERRE3: the reference's products of basis
+// values — upper Gram (10), right-hand side (4), count — 15 sums.  POLY_SV: every
+// Gram entry of {1, x, x^2, x^3, w, x w} is a monomial x^a w^c, so the thread keeps
+// the 15 distinct monomial sums (x^0..x^6, w x^0..x^4, w^2 x^0..x^2) and the 6
+// right-hand sides, 21 sums, expanded to the Gram before the solve.
+template <int BASIS>
+struct AccTraits;
+template <>
+struct AccTraits<QK_LSM_LAGUERRE3> {
+    static constexpr int N = 15;
+};
+template <>
+struct AccTraits<QK_LSM_POLY_SV> {
+    static constexpr int N = 21;
+};
+
+template <class R, int BASIS>
+__device__ __forceinline__ void accumulate(double *acc, R S, R v, R K, double inv_K, double cx, double cv, R Y) {
+    const double y = static_cast<double>(Y);
+    if constexpr (BASIS == QK_LSM_LAGUERRE3) {
+        R b[4];
+        laguerre_basis<R>(S, K, b);
+        int j = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const double br = static_cast<double>(b[r]);
+#pragma unroll
+            for (int q = r; q < 4; ++q) acc[j++] += br * static_cast<double>(b[q]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[j++] += static_cast<double>(b[r]) * y;
+        acc[j] += 1.0;
+    } else {
+        const PolyPoint q = poly_point<R>(S, v, inv_K, cx, cv);
+        const double x = q.x, w = q.w;
+        const double x2 = x * x, x3 = x2 * x, ww = w * w;
+        acc[0] += 1.0;
+        acc[1] += x;
+        acc[2] += x2;
+        acc[3] += x3;
+        acc[4] += x2 * x2;
+        acc[5] += x2 * x3;
+        acc[6] += x3 * x3;
+        acc[7] += w;
+        acc[8] += w * x;
+        acc[9] += w * x2;
+        acc[10] += w * x3;
+        acc[11] += w * x2 * x2;
+        acc[12] += ww;
+        acc[13] += ww * x;
+        acc[14] += ww * x2;
+        acc[15] += y;
+        acc[16] += y * x;
+        acc[17] += y * x2;
+        acc[18] += y * x3;
+        acc[19] += y * w;
+        acc[20] += y * x * w;
+    }
+}
+
+// The solver's input: upper Gram (row-major), right-hand side, count.
+template <int BASIS>
+__device__ __forceinline__ void expand_sums(const double *acc, double *sums) {
+    if constexpr (BASIS == QK_LSM_LAGUERRE3) {
+        for (int j = 0; j < AccTraits<BASIS>::N; ++j) sums[j] = acc[j];
+    } else {
+        // basis i = x^pa[i] w^pc[i]
+        const int pa[6] = {0, 1, 2, 3, 0, 1};
+        const int pc[6] = {0, 0, 0, 0, 1, 1};
+        int j = 0;
+        for (int r = 0; r < 6; ++r)
+            for (int q = r; q < 6; ++q) {
+                const int a = pa[r] + pa[q], c = pc[r] + pc[q];
+                sums[j++] = c == 0 ? acc[a] : (c == 1 ? acc[7 + a] : acc[12 + a]);
+            }
+        for (int r = 0; r < 6; ++r) sums[j++] = pc[r] == 0 ? acc[15 + pa[r]] : acc[19 + pa[r]];
+        sums[j] = acc[0];
+    }
 }
 
 // ---------------------------------------------------------------- FP64 solves
@@ -284,15 +371,44 @@ __device__ int solve_scaled(const double *sums, double *c) {
     return 1;
 }
 
-// Four consecutive slab entries (rows are 16-byte aligned: ld is a multiple of 4).
+// ---------------------------------------------------------------- streaming
+// cp.async (16 bytes, L2 only) into shared memory with an L2 eviction-priority
+// hint; completion is tracked per thread with commit/wait groups (no spin).
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, uint64_t policy) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "l"(policy)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+constexpr int kLsmChunk = 4 * kLsmBlock;  // paths per staged chunk: four per thread
+
+// Four consecutive entries at a 16-byte aligned address (shared or global).
 __device__ __forceinline__ void load4(const float *p, float v[4]) {
     const float4 q = *reinterpret_cast<const float4 *>(p);
-    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
 }
 __device__ __forceinline__ void load4(const double *p, double v[4]) {
     const double2 a = *reinterpret_cast<const double2 *>(p);
     const double2 b = *reinterpret_cast<const double2 *>(p + 2);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
 }
 __device__ __forceinline__ void store4(float *p, const float v[4]) {
     *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
@@ -302,16 +418,34 @@ __device__ __forceinline__ void store4(double *p, const double v[4]) {
     *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
 }
 
+// Shared-memory slots of one stage: spot at the update date, cash flows, spot at
+// the Gram date, then (POLY_SV) variance at both dates.
+template <int BASIS>
+struct StageLayout {
+    static constexpr int kArrays = BASIS == QK_LSM_POLY_SV ? 5 : 3;
+    static constexpr int kSu = 0, kCf = 1, kSg = 2, kVu = 3, kVg = 4;
+};
+
+template <class R, int BASIS>
+constexpr size_t lsm_sweep_smem() {
+    return 2 * StageLayout<BASIS>::kArrays * kLsmChunk * sizeof(R);
+}
+
 // Backward sweep over one date pair.  init: cash flows start as the payoff at
 // date d_upd (maturity); otherwise the exercise decision of date d_upd is
 // applied with its solved coefficients.  Then, if d_gram >= 0, the ITM
 // regression sums of date d_gram are accumulated with Y = cf * disc, reduced per
 // block, and the last block to finish (counted on `done`) reduces all block sums
 // in a fixed order and solves date d_gram's coefficients — no separate launch and
-// no wait: every other block simply exits.  Each thread handles groups of four
-// consecutive paths with 16-byte loads.
+// no wait: every other block simply exits.
+//
+// Each block streams chunks of kLsmChunk paths (its chunks are blockIdx.x +
+// k * gridDim.x) through two shared-memory stages: while chunk k is processed the
+// copies of chunk k+1 are in flight.  The spot/variance rows of the update date are
+// read for the last time here (L2 evict-first); those of the Gram date are read
+// again by the next date's launch (L2 evict-last), so they are served from L2.
 template <class R, int BASIS>
-__global__ void __launch_bounds__(kLsmBlock, 2) lsm_sweep_kernel(LsmArgs a, const R *__restrict__ slab_S,
+__global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel(LsmArgs a, const R *__restrict__ slab_S,
                                                              const R *__restrict__ slab_v, R *__restrict__ cf,
                                                              int d_upd, int init, int d_gram,
                                                              double *__restrict__ coeffs,
@@ -320,12 +454,22 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_sweep_kernel(LsmArgs a, cons
                                                              unsigned int *__restrict__ done, int *__restrict__ flags) {
     constexpr int NB = BasisTraits<BASIS>::NB;
     constexpr int NSUM = Sums<NB>::NSUM;
+    constexpr int NACC = AccTraits<BASIS>::N;
+    constexpr bool use_v = BASIS == QK_LSM_POLY_SV;
+    using L = StageLayout<BASIS>;
+    extern __shared__ __align__(16) unsigned char lsm_smem[];
+    R *stage = reinterpret_cast<R *>(lsm_smem);
+
     const R K = static_cast<R>(a.K);
+    const double inv_K = 1.0 / a.K;
     const R disc = static_cast<R>(a.disc);
-    double acc[NSUM];
+    const bool gram = d_gram >= 0;
+    double acc[NACC];
 #pragma unroll
-    for (int j = 0; j < NSUM; ++j) acc[j] = 0.0;
+    for (int j = 0; j < NACC; ++j) acc[j] = 0.0;
     double cu[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) cu[i] = 0.0;
     double cxu = 0.0, cvu = 0.0, cxg = 0.0, cvg = 0.0;
     if (!init) {
 #pragma unroll
@@ -333,79 +477,99 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_sweep_kernel(LsmArgs a, cons
         cxu = centre[2 * d_upd];
         cvu = centre[2 * d_upd + 1];
     }
-    if (d_gram >= 0) {
+    if (gram) {
         cxg = centre[2 * d_gram];
         cvg = centre[2 * d_gram + 1];
     }
-    constexpr bool use_v = BASIS == QK_LSM_POLY_SV;
-    const int64_t groups = a.ld / 4;
-    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     const R *Su = slab_S + static_cast<int64_t>(d_upd) * a.ld;
     const R *Vu = use_v ? slab_v + static_cast<int64_t>(d_upd) * a.ld : nullptr;
-    const R *Sg = slab_S + static_cast<int64_t>(d_gram < 0 ? 0 : d_gram) * a.ld;
-    const R *Vg = use_v ? slab_v + static_cast<int64_t>(d_gram < 0 ? 0 : d_gram) * a.ld : nullptr;
-    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < groups; g += stride) {
-        const int64_t i0 = 4 * g;
-        R S4[4], c4[4], v4[4] = {R(0), R(0), R(0), R(0)};
-        load4(Su + i0, S4);
-        if (use_v) load4(Vu + i0, v4);
-        if (!init) load4(cf + i0, c4);
+    const R *Sg = slab_S + static_cast<int64_t>(gram ? d_gram : 0) * a.ld;
+    const R *Vg = use_v ? slab_v + static_cast<int64_t>(gram ? d_gram : 0) * a.ld : nullptr;
+    const uint64_t pol_first = l2_policy_evict_first();
+    const uint64_t pol_last = l2_policy_evict_last();
+    const int64_t n_chunks = (a.ld + kLsmChunk - 1) / kLsmChunk;
+    constexpr int kPer16 = 16 / static_cast<int>(sizeof(R));  // elements per 16-byte copy
+
+    // Queue the copies of one chunk into stage st.  Rows hold ld elements, ld a
+    // multiple of 4, so no 16-byte group straddles the end of a row.
+    auto issue = [&](int64_t chunk, int st) {
+        R *base = stage + static_cast<size_t>(st) * L::kArrays * kLsmChunk;
+        const int64_t p0 = chunk * kLsmChunk;
+        for (int e = threadIdx.x * kPer16; e < kLsmChunk; e += kLsmBlock * kPer16) {
+            const int64_t i = p0 + e;
+            if (i >= a.ld) break;
+            cp_async16(base + L::kSu * kLsmChunk + e, Su + i, pol_first);
+            if (!init) cp_async16(base + L::kCf * kLsmChunk + e, cf + i, pol_last);
+            if (gram) cp_async16(base + L::kSg * kLsmChunk + e, Sg + i, pol_last);
+            if constexpr (use_v) {
+                cp_async16(base + L::kVu * kLsmChunk + e, Vu + i, pol_first);
+                if (gram) cp_async16(base + L::kVg * kLsmChunk + e, Vg + i, pol_last);
+            }
+        }
+    };
+
+    int64_t chunk = blockIdx.x;
+    if (chunk < n_chunks) issue(chunk, 0);
+    cp_async_commit();
+    for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {
+        const int64_t next = chunk + gridDim.x;
+        if (next < n_chunks) issue(next, (k + 1) & 1);
+        cp_async_commit();
+        cp_async_wait_all_but_one();  // this thread's copies of `chunk` have landed
+        __syncthreads();              // ... and every other thread's
+        const R *base = stage + static_cast<size_t>(k & 1) * L::kArrays * kLsmChunk;
+        // four consecutive paths per thread: 16-byte shared loads, no bank conflicts
+        const int j0 = 4 * threadIdx.x;
+        const int64_t i0 = chunk * kLsmChunk + j0;
+        if (i0 < a.N) {
+            R S4[4], c4[4], v4[4] = {R(0), R(0), R(0), R(0)};
+            load4(base + L::kSu * kLsmChunk + j0, S4);
+            if (!init) load4(base + L::kCf * kLsmChunk + j0, c4);
+            if (use_v) load4(base + L::kVu * kLsmChunk + j0, v4);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const R iv = lsm_intrinsic<R>(a.right, S4[k], K);
-            if (init) {
-                c4[k] = iv;
-            } else {
-                const R disc_c = c4[k] * disc;
-                if (iv > R(0)) {
-                    const double hold = continuation<R, BASIS>(cu, S4[k], v4[k], K, cxu, cvu);
-                    c4[k] = (static_cast<double>(iv) > hold) ? iv : disc_c;
+            for (int q = 0; q < 4; ++q) {
+                const R iv = lsm_intrinsic<R>(a.right, S4[q], K);
+                if (init) {
+                    c4[q] = iv;
                 } else {
-                    c4[k] = disc_c;
-                }
-            }
-        }
-        store4(cf + i0, c4);
-        if (d_gram >= 0) {
-            R Sg4[4], vg4[4] = {R(0), R(0), R(0), R(0)};
-            load4(Sg + i0, Sg4);
-            if (use_v) load4(Vg + i0, vg4);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const R ivg = lsm_intrinsic<R>(a.right, Sg4[k], K);
-                if (ivg > R(0) && i0 + k < a.N) {
-                    const R Y = c4[k] * disc;
-                    R b[NB];
-                    eval_basis<R, BASIS>(Sg4[k], vg4[k], K, cxg, cvg, b);
-                    int j = 0;
-#pragma unroll
-                    for (int r = 0; r < NB; ++r) {
-                        const double br = static_cast<double>(b[r]);
-#pragma unroll
-                        for (int q = r; q < NB; ++q) acc[j++] += br * static_cast<double>(b[q]);
+                    const R disc_c = c4[q] * disc;
+                    R c = disc_c;
+                    if (iv > R(0)) {
+                        const double hold = continuation<R, BASIS>(cu, S4[q], v4[q], K, inv_K, cxu, cvu);
+                        if (static_cast<double>(iv) > hold) c = iv;
                     }
+                    c4[q] = c;
+                }
+            }
+            store4(cf + i0, c4);  // i0 + 3 < ld: rows are padded to a multiple of 4
+            if (gram) {
+                R Sg4[4], vg4[4] = {R(0), R(0), R(0), R(0)};
+                load4(base + L::kSg * kLsmChunk + j0, Sg4);
+                if (use_v) load4(base + L::kVg * kLsmChunk + j0, vg4);
 #pragma unroll
-                    for (int r = 0; r < NB; ++r) acc[j++] += static_cast<double>(b[r]) * static_cast<double>(Y);
-                    acc[j] += 1.0;
+                for (int q = 0; q < 4; ++q) {
+                    if (i0 + q < a.N && lsm_intrinsic<R>(a.right, Sg4[q], K) > R(0))
+                        accumulate<R, BASIS>(acc, Sg4[q], vg4[q], K, inv_K, cxg, cvg, c4[q] * disc);
                 }
             }
         }
+        __syncthreads();  // the stage is refilled by the next iteration's copies
     }
-    if (d_gram < 0) return;
-    // block reduction of the NSUM sums
-    __shared__ double s_red[kLsmBlock / 32][NSUM];
+    if (!gram) return;
+    // block reduction of the NACC sums
+    __shared__ double s_red[kLsmBlock / 32][NACC];
     __shared__ bool s_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j < NSUM; ++j) {
+    for (int j = 0; j < NACC; ++j) {
         const double v = warp_sum(acc[j]);
         if (lane == 0) s_red[warp][j] = v;
     }
     __syncthreads();
-    if (threadIdx.x < NSUM) {
+    if (threadIdx.x < NACC) {
         double t = 0.0;
         for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red[w][threadIdx.x];
-        block_sums[static_cast<int64_t>(blockIdx.x) * NSUM + threadIdx.x] = t;
+        block_sums[static_cast<int64_t>(blockIdx.x) * NACC + threadIdx.x] = t;
         __threadfence();  // this block's sums are visible device-wide before it is counted
     }
     __syncthreads();
@@ -414,21 +578,23 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_sweep_kernel(LsmArgs a, cons
     if (!s_last) return;
     // last block: fixed-order reduction of all block sums, then the FP64 solve
     __threadfence();
-    __shared__ double s_part[kLsmBlock / 32][NSUM];
-    if (warp < kLsmBlock / 32 && lane < NSUM) {
+    __shared__ double s_part[kLsmBlock / 32][NACC];
+    if (lane < NACC) {
         double t = 0.0;
         for (int b = warp; b < static_cast<int>(gridDim.x); b += kLsmBlock / 32)
-            t += __ldcg(block_sums + static_cast<int64_t>(b) * NSUM + lane);
+            t += __ldcg(block_sums + static_cast<int64_t>(b) * NACC + lane);
         s_part[warp][lane] = t;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double sums[NSUM];
-        for (int j = 0; j < NSUM; ++j) {
+        double tot[NACC];
+        for (int j = 0; j < NACC; ++j) {
             double t = 0.0;
             for (int w = 0; w < kLsmBlock / 32; ++w) t += s_part[w][j];
-            sums[j] = t;
+            tot[j] = t;
         }
+        double sums[NSUM];
+        expand_sums<BASIS>(tot, sums);
         double c[NB];
         const int f = (BASIS == QK_LSM_LAGUERRE3) ? solve_reference<NB>(sums, c) : solve_scaled<NB>(sums, c);
         for (int i = 0; i < kMaxCoef; ++i) coeffs[d_gram * kMaxCoef + i] = i < NB ? c[i] : 0.0;
@@ -453,6 +619,7 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_final_kernel(LsmArgs a, const R
     double cu[NB];
     for (int i = 0; i < NB; ++i) cu[i] = init ? 0.0 : coeffs[i];
     const double cx = centre[0], cv = centre[1];
+    const double inv_K = 1.0 / a.K;
     const bool use_v = BASIS == QK_LSM_POLY_SV;
     __shared__ Moments s_warp[kLsmBlock / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -474,7 +641,7 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_final_kernel(LsmArgs a, const R
                 const R disc_c = c * disc;
                 if (iv > R(0)) {
                     const R v = use_v ? slab_v[i] : R(0);
-                    const double hold = continuation<R, BASIS>(cu, S, v, K, cx, cv);
+                    const double hold = continuation<R, BASIS>(cu, S, v, K, inv_K, cx, cv);
                     c = (static_cast<double>(iv) > hold) ? iv : disc_c;
                 } else {
                     c = disc_c;
@@ -508,7 +675,7 @@ namespace {
     } while (0)
 
 template <class R, int BASIS>
-cudaError_t enqueue_backward(cudaStream_t s, int grid, const LsmArgs &a, const R *S, const R *V, R *cf,
+cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmArgs &a, const R *S, const R *V, R *cf,
                              double *coeffs, int *flags, const double *centre, double *block_sums,
                              unsigned int *done, Moments *block_moments, int64_t *launches) {
     const int D = a.n_dates;
@@ -517,14 +684,24 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, const LsmArgs &a, const R
         ++*launches;
         return cudaGetLastError();
     }
-    cudaError_t e = cudaMemsetAsync(done, 0, sizeof(unsigned int), s);
+    // sweep grid: every resident block slot of the GPU (at most 4 per SM; the
+    // block-sum arena holds 4 * sm_count * 32 doubles)
+    const size_t smem = lsm_sweep_smem<R, BASIS>();
+    cudaError_t e = cudaFuncSetAttribute(lsm_sweep_kernel<R, BASIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre, block_sums,
-                                                          done, flags);
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_sweep_kernel<R, BASIS>, kLsmBlock, smem);
+    if (e != cudaSuccess) return e;
+    const int sgrid = sm_count * std::min(std::max(per_sm, 1), 4);
+    e = cudaMemsetAsync(done, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    lsm_sweep_kernel<R, BASIS><<<sgrid, kLsmBlock, smem, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre,
+                                                              block_sums, done, flags);
     ++*launches;
     for (int d = D - 2; d >= 1; --d) {
-        lsm_sweep_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, d, 0, d - 1, coeffs, centre, block_sums,
-                                                              done, flags);
+        lsm_sweep_kernel<R, BASIS><<<sgrid, kLsmBlock, smem, s>>>(a, S, V, cf, d, 0, d - 1, coeffs, centre,
+                                                                  block_sums, done, flags);
         ++*launches;
     }
     lsm_final_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, 0, coeffs, centre, block_moments);
@@ -604,7 +781,7 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
     for (const Job &j : jobs) any_v |= j.b.lsm_basis == QK_LSM_POLY_SV;
     if (any_v && (st = L.slab_v.ensure(max_slab)) != QK_OK) return st;
     if ((st = L.cashflow.ensure(max_cf)) != QK_OK) return st;
-    if ((st = L.block_sums.ensure(static_cast<size_t>(grid) * 64 * sizeof(double))) != QK_OK) return st;
+    if ((st = L.block_sums.ensure(static_cast<size_t>(h->sm_count) * 4 * 32 * sizeof(double))) != QK_OK) return st;
     if ((st = L.coeffs.ensure(static_cast<size_t>(max_dates) * kMaxCoef * sizeof(double) + 2 * max_dates * sizeof(double) * nj + 64)) != QK_OK) return st;
     if ((st = L.status.ensure(static_cast<size_t>(max_dates) * sizeof(int) + 256)) != QK_OK) return st;
     if ((st = lsm_events_ensure(h, 3 * nj)) != QK_OK) return st;
@@ -664,22 +841,22 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         cudaError_t e;
         if (prec == QK_FP32) {
             if (use_v)
-                e = enqueue_backward<float, QK_LSM_POLY_SV>(h->stream, grid, a, static_cast<const float *>(L.slab_S.ptr),
+                e = enqueue_backward<float, QK_LSM_POLY_SV>(h->stream, grid, h->sm_count, a, static_cast<const float *>(L.slab_S.ptr),
                                                            static_cast<const float *>(L.slab_v.ptr),
                                                            static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, done, bm,
                                                            &h->lsm_launches);
             else
-                e = enqueue_backward<float, QK_LSM_LAGUERRE3>(h->stream, grid, a, static_cast<const float *>(L.slab_S.ptr),
+                e = enqueue_backward<float, QK_LSM_LAGUERRE3>(h->stream, grid, h->sm_count, a, static_cast<const float *>(L.slab_S.ptr),
                                                              nullptr, static_cast<float *>(L.cashflow.ptr), d_coeffs, fl,
                                                              cen, bs, done, bm, &h->lsm_launches);
         } else {
             if (use_v)
-                e = enqueue_backward<double, QK_LSM_POLY_SV>(h->stream, grid, a, static_cast<const double *>(L.slab_S.ptr),
+                e = enqueue_backward<double, QK_LSM_POLY_SV>(h->stream, grid, h->sm_count, a, static_cast<const double *>(L.slab_S.ptr),
                                                             static_cast<const double *>(L.slab_v.ptr),
                                                             static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen, bs,
                                                             done, bm, &h->lsm_launches);
             else
-                e = enqueue_backward<double, QK_LSM_LAGUERRE3>(h->stream, grid, a,
+                e = enqueue_backward<double, QK_LSM_LAGUERRE3>(h->stream, grid, h->sm_count, a,
                                                               static_cast<const double *>(L.slab_S.ptr), nullptr,
                                                               static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen,
                                                               bs, done, bm, &h->lsm_launches);

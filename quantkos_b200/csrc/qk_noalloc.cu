@@ -82,6 +82,7 @@ extern "C" qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_res
     for (int k = 0; k < c->n_payoffs; ++k)
         if (c->payoffs[k].type == QK_AMERICAN)
             return qk::fail(QK_ERR_UNSUPPORTED, "qk_price_noalloc: American contracts need LSM slabs; use qk_price_batch");
+    if (c->antithetic) return qk::fail(QK_ERR_UNSUPPORTED, "qk_price_noalloc: antithetic pairs go through qk_price_batch");
     const int64_t tiles = (c->n_paths + kNoAllocPathsPerTile - 1) / kNoAllocPathsPerTile;
     if (static_cast<size_t>(tiles) * c->n_payoffs > kNoAllocMaxRecords)
         return qk::fail(QK_ERR_CAPACITY, "qk_price_noalloc: ceil(n_paths / 2048) * n_payoffs = " +

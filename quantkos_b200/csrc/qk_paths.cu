@@ -32,14 +32,16 @@ struct SlabSink {
     R *slab_S;
     R *slab_v;
     int64_t ld;     // leading dimension (paths per slab row)
-    int64_t col;    // this path's column
+    int64_t pos;    // slab index of this path's next stored date: row * ld + column
     int stride;     // steps between stored dates
-    __device__ __forceinline__ void operator()(int n, R S, R v) const {
-        const int np1 = n + 1;
-        if (np1 % stride == 0) {
-            const int64_t row = np1 / stride - 1;
-            slab_S[row * ld + col] = S;
-            if (slab_v) slab_v[row * ld + col] = v;
+    int left;       // steps until the next stored date
+    // Called once per step, in order: every stride-th step is stored.
+    __device__ __forceinline__ void operator()(int, R S, R v) {
+        if (--left == 0) {
+            left = stride;
+            slab_S[pos] = S;
+            if (slab_v) slab_v[pos] = v;
+            pos += ld;
         }
     }
 };
@@ -96,7 +98,7 @@ __device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st
 template <class R, int MODEL, int SCHEME, class Gen, class Sink>
 __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
                                               uint32_t k0, uint32_t k1, uint32_t path, uint32_t stream, uint32_t kmin,
-                                              PathState<R> &st, const Sink &sink) {
+                                              PathState<R> &st, Sink &&sink) {
     st.S = S0;
     st.v = v0;
     st.ssum = 0.0;
@@ -133,6 +135,68 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
     }
 }
 
+// Antithetic pair: one set of draws, the second path with every normal negated.
+template <class R, int MODEL, int SCHEME>
+__device__ __forceinline__ void one_step_pair(const StepConst<R> &p, PathState<R> &a, PathState<R> &b, uint32_t wa,
+                                              uint32_t wb, uint32_t wpois, uint32_t kmin, uint32_t k0, uint32_t k1,
+                                              uint32_t path, uint32_t stream, int n) {
+    R z1, z2;
+    Math<R>::box_muller(wa, wb, z1, z2);
+    heston_step<R, SCHEME>(p, a.S, a.v, z1, z2);
+    heston_step<R, SCHEME>(p, b.S, b.v, -z1, -z2);
+    if constexpr (MODEL == kBates) {
+        if (jump_test<R>(wpois, p, kmin)) {
+            PhiloxJumpDraws<R> d{k0, k1, path, stream, static_cast<uint32_t>(n), Math<R>::u01(wpois), 1, 0, U4{0, 0, 0, 0}};
+            R fa, fb;
+            jump_factor_pair<R>(p, d.first, d, fa, fb);
+            a.S *= fa;
+            b.S *= fb;
+        }
+    }
+}
+
+template <class R, int MODEL, int SCHEME, class Gen>
+__device__ __forceinline__ void simulate_pair(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
+                                              uint32_t k0, uint32_t k1, uint32_t pair, uint32_t stream, uint32_t kmin,
+                                              PathState<R> &a, PathState<R> &b) {
+    a.S = b.S = S0;
+    a.v = b.v = v0;
+    a.ssum = b.ssum = 0.0;
+    a.smax = b.smax = S0;
+    a.smin = b.smin = S0;
+    for (int n0 = 0; n0 < n_steps; n0 += kSumChunk) {
+        const int n1 = min(n0 + kSumChunk, n_steps);
+        R blk_a = R(0), blk_b = R(0);
+        U4 wp{0u, 0u, 0u, 0u};
+        int n = n0;
+        for (; n + 1 < n1; n += 2) {
+            const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), pair, stream, 0u});
+            if constexpr (MODEL == kBates) {
+                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), pair, stream, 2u});
+            }
+            const bool lo = (n & 3) == 0;
+            one_step_pair<R, MODEL, SCHEME>(p, a, b, w.x, w.y, lo ? wp.x : wp.z, kmin, k0, k1, pair, stream, n);
+            track(a, blk_a);
+            track(b, blk_b);
+            one_step_pair<R, MODEL, SCHEME>(p, a, b, w.z, w.w, lo ? wp.y : wp.w, kmin, k0, k1, pair, stream, n + 1);
+            track(a, blk_a);
+            track(b, blk_b);
+        }
+        if (n < n1) {
+            const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), pair, stream, 0u});
+            if constexpr (MODEL == kBates) {
+                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), pair, stream, 2u});
+            }
+            one_step_pair<R, MODEL, SCHEME>(p, a, b, w.x, w.y, (n & 3) == 0 ? wp.x : wp.z, kmin, k0, k1, pair, stream,
+                                            n);
+            track(a, blk_a);
+            track(b, blk_b);
+        }
+        a.ssum += static_cast<double>(blk_a);
+        b.ssum += static_cast<double>(blk_b);
+    }
+}
+
 template <class R>
 __device__ __forceinline__ const StepConst<R> &task_const(const TaskDev &t);
 template <>
@@ -142,7 +206,7 @@ __device__ __forceinline__ const StepConst<double> &task_const<double>(const Tas
 
 template <class R, class Sink>
 __device__ __forceinline__ void simulate_dispatch(const TaskDev &t, const StepConst<R> &p, uint32_t path,
-                                                  PathState<R> &st, const Sink &sink) {
+                                                  PathState<R> &st, Sink &&sink) {
     const R S0 = static_cast<R>(t.S0);
     const R v0 = static_cast<R>(t.v0);
     const uint32_t km = t.jump_kmin;
@@ -176,7 +240,7 @@ __device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int
     return lo;
 }
 
-template <class R, int MODEL, int SCHEME, bool UK>
+template <class R, int MODEL, int SCHEME, bool UK, bool ANTI>
 __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp32 : 1)
     price_tiles_kernel(const TaskDev *__restrict__ tasks, const int64_t *__restrict__ prefix, int32_t n_tasks,
                        int64_t slot_begin, int64_t slot_end, unsigned long long *__restrict__ cursor,
@@ -201,39 +265,69 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
         const int64_t tile = q - t.tile_begin;
         const StepConst<R> p = task_const<R>(t);
         const int np = t.n_payoffs;
-        const int ppt = t.ppt;
         const int n_steps = t.n_steps;
         const int64_t n_paths = t.n_paths;
         const uint32_t k0 = t.key0, k1 = t.key1, stream = t.stream, kmin = t.jump_kmin;
         const R S0 = static_cast<R>(t.S0), v0 = static_cast<R>(t.v0);
-        const int64_t tile_first = tile * static_cast<int64_t>(kWarpTilePaths) * ppt;
+        // big tiles of ppt rounds, then the tail in tiles of ppt_tail rounds
+        const bool big = tile < t.n_big;
+        const int tile_rounds = big ? t.ppt : t.ppt_tail;
+        const int64_t first_round = big ? tile * t.ppt
+                                        : static_cast<int64_t>(t.n_big) * t.ppt + (tile - t.n_big) * t.ppt_tail;
+        const int64_t tile_first = first_round * kWarpTilePaths;
         if (lane < np) acc[lane] = Moments{0.0, 0.0, 0.0, 0.0};
         __syncwarp();
 
-        const int64_t left = n_paths - tile_first;
+        // a lane's unit is one path, or one antithetic pair of paths
+        const int64_t n_units = ANTI ? (n_paths >> 1) : n_paths;
+        const int64_t left = n_units - tile_first;
         const int rounds =
-            static_cast<int>(min(static_cast<int64_t>(ppt), (left + kWarpTilePaths - 1) / kWarpTilePaths));
+            static_cast<int>(min(static_cast<int64_t>(tile_rounds), (left + kWarpTilePaths - 1) / kWarpTilePaths));
         for (int j = 0; j < rounds; ++j) {
-            const int64_t path = tile_first + static_cast<int64_t>(j) * kWarpTilePaths + lane;
-            const bool active = path < n_paths;
-            PathState<R> st;
-            if (active) {
-                if constexpr (UK) {
-                    simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
-                                                    static_cast<uint32_t>(path), stream, kmin, st, NoSink{});
+            const int64_t unit = tile_first + static_cast<int64_t>(j) * kWarpTilePaths + lane;
+            const bool active = unit < n_units;
+            if constexpr (ANTI) {
+                PathState<R> sa, sb;
+                if (active) {
+                    if constexpr (UK) {
+                        simulate_pair<R, MODEL, SCHEME>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
+                                                        static_cast<uint32_t>(unit), stream, kmin, sa, sb);
+                    } else {
+                        simulate_pair<R, MODEL, SCHEME>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
+                                                        static_cast<uint32_t>(unit), stream, kmin, sa, sb);
+                    }
                 } else {
-                    simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
-                                                    static_cast<uint32_t>(path), stream, kmin, st, NoSink{});
+                    sa.S = sa.smax = sa.smin = sb.S = sb.smax = sb.smin = R(0);
+                    sa.ssum = sb.ssum = 0.0;
+                }
+                for (int k = 0; k < np; ++k) {
+                    const PayoffSpec ps = t.pay[k];
+                    const R xa = active ? final_payoff<R>(ps, sa.S, sa.ssum, sa.smax, sa.smin, n_steps) : R(0);
+                    const R xb = active ? final_payoff<R>(ps, sb.S, sb.ssum, sb.smax, sb.smin, n_steps) : R(0);
+                    const double y = 0.5 * (static_cast<double>(xa) + static_cast<double>(xb));
+                    const Moments wm = warp_moments_pair(y, active, xa > eps_payoff, xb > eps_payoff);
+                    if (lane == 0) acc[k] = chan_merge(acc[k], wm);
                 }
             } else {
-                st.S = st.smax = st.smin = R(0);
-                st.ssum = 0.0;
-            }
-            for (int k = 0; k < np; ++k) {
-                const PayoffSpec ps = t.pay[k];
-                const R x = active ? final_payoff<R>(ps, st.S, st.ssum, st.smax, st.smin, n_steps) : R(0);
-                const Moments wm = warp_moments(static_cast<double>(x), active, x > eps_payoff);
-                if (lane == 0) acc[k] = chan_merge(acc[k], wm);
+                PathState<R> st;
+                if (active) {
+                    if constexpr (UK) {
+                        simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
+                                                        static_cast<uint32_t>(unit), stream, kmin, st, NoSink{});
+                    } else {
+                        simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
+                                                        static_cast<uint32_t>(unit), stream, kmin, st, NoSink{});
+                    }
+                } else {
+                    st.S = st.smax = st.smin = R(0);
+                    st.ssum = 0.0;
+                }
+                for (int k = 0; k < np; ++k) {
+                    const PayoffSpec ps = t.pay[k];
+                    const R x = active ? final_payoff<R>(ps, st.S, st.ssum, st.smax, st.smin, n_steps) : R(0);
+                    const Moments wm = warp_moments(static_cast<double>(x), active, x > eps_payoff);
+                    if (lane == 0) acc[k] = chan_merge(acc[k], wm);
+                }
             }
         }
         __syncwarp();
@@ -246,30 +340,35 @@ template <class R>
 using PriceKernel = void (*)(const TaskDev *, const int64_t *, int32_t, int64_t, int64_t, unsigned long long *,
                              Moments *, const PhiloxRoundKeys);
 
-template <class R, bool UK>
+template <class R, bool UK, bool ANTI>
 __host__ PriceKernel<R> price_kernel_for_keys(int model, int scheme) {
     switch (model * 3 + scheme) {
-        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK>;
-        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK>;
-        case 2: return price_tiles_kernel<R, kHeston, kQE, UK>;
-        case 3: return price_tiles_kernel<R, kBates, kEuler, UK>;
-        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK>;
-        default: return price_tiles_kernel<R, kBates, kQE, UK>;
+        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK, ANTI>;
+        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK, ANTI>;
+        case 2: return price_tiles_kernel<R, kHeston, kQE, UK, ANTI>;
+        case 3: return price_tiles_kernel<R, kBates, kEuler, UK, ANTI>;
+        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK, ANTI>;
+        default: return price_tiles_kernel<R, kBates, kQE, UK, ANTI>;
     }
 }
 
 template <class R>
-__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true) {
-    return uniform_key ? price_kernel_for_keys<R, true>(model, scheme) : price_kernel_for_keys<R, false>(model, scheme);
+__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true, bool antithetic = false) {
+    if (antithetic)
+        return uniform_key ? price_kernel_for_keys<R, true, true>(model, scheme)
+                           : price_kernel_for_keys<R, false, true>(model, scheme);
+    return uniform_key ? price_kernel_for_keys<R, true, false>(model, scheme)
+                       : price_kernel_for_keys<R, false, false>(model, scheme);
 }
 
-// Per task and leg: merge the task's tile moments in one pass about a shift c
-// (the first tile's mean).  With d_i = mean_i - c:  N = sum n_i,  D = sum n_i d_i,
-// Q = sum (M2_i + n_i d_i^2), then mean = c + D / N and M2 = Q - D^2 / N (the
-// pairwise update of Chan et al. applied to all tiles at once; c lies within a
-// few standard errors of the mean, so D^2 / N is a small correction to Q).  No
-// division per record; per-thread sums fold through a fixed-shape tree, so the
-// result is deterministic for a given tile plan.
+// Merging moment records.  A set of records (n_i, mean_i, M2_i, itm_i) is merged
+// in one pass about a shift c (the first record's mean).  With d_i = mean_i - c:
+// N = sum n_i,  D = sum n_i d_i,  Q = sum (M2_i + n_i d_i^2), then
+// mean = c + D / N and M2 = Q - D^2 / N (the pairwise update of Chan et al.
+// applied to all records at once; c lies within a few standard errors of the
+// mean, so D^2 / N is a small correction to Q).  No division per record;
+// per-thread sums fold through a fixed-shape tree, so the result is deterministic
+// for a given tile plan.
 __device__ __forceinline__ void block_sum4(double &a, double &b, double &c, double &d, double (*red)[32]) {
     a = warp_sum(a);
     b = warp_sum(b);
@@ -296,37 +395,79 @@ __device__ __forceinline__ void block_sum4(double &a, double &b, double &c, doub
     __syncthreads();
 }
 
+// Block-wide merge of rec[i * stride], i < count; the result is valid in thread 0.
+__device__ __forceinline__ Moments merge_range(const Moments *__restrict__ rec, int64_t count, int64_t stride,
+                                               double (*red)[32]) {
+    const double c = count > 0 ? rec[0].mean : 0.0;
+    double n = 0.0, D = 0.0, Q = 0.0, itm = 0.0;
+    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) {
+        const Moments m = rec[i * stride];
+        const double d = m.mean - c;
+        const double nd = m.n * d;
+        n += m.n;
+        D += nd;
+        Q += fma(nd, d, m.m2);
+        itm += m.itm;
+    }
+    block_sum4(n, D, Q, itm, red);
+    Moments r{0.0, 0.0, 0.0, 0.0};
+    if (n > 0.0) {
+        r.n = n;
+        r.mean = c + D / n;
+        r.m2 = fmax(Q - D * (D / n), 0.0);
+        r.itm = itm;
+    }
+    return r;
+}
+
+// One block per task: merge all its tile records (tasks with few tiles; the
+// allocation-free entry point).
 __global__ void __launch_bounds__(1024) merge_tasks_kernel(const TaskDev *__restrict__ tasks,
                                                            const Moments *__restrict__ partials,
                                                            TaskMoments *__restrict__ out) {
     __shared__ double red[4][32];
     const TaskDev &t = tasks[blockIdx.x];
     const int np = t.n_payoffs;
-    const int64_t n_tiles = t.n_tiles;
-    const Moments *rec = partials + t.partial_base;
     for (int k = 0; k < np; ++k) {
-        const double c = n_tiles > 0 ? rec[k].mean : 0.0;
-        double n = 0.0, D = 0.0, Q = 0.0, itm = 0.0;
-        for (int64_t i = threadIdx.x; i < n_tiles; i += blockDim.x) {
-            const Moments m = rec[i * np + k];
-            const double d = m.mean - c;
-            const double nd = m.n * d;
-            n += m.n;
-            D += nd;
-            Q += fma(nd, d, m.m2);
-            itm += m.itm;
-        }
-        block_sum4(n, D, Q, itm, red);
-        if (threadIdx.x == 0) {
-            Moments r{0.0, 0.0, 0.0, 0.0};
-            if (n > 0.0) {
-                r.n = n;
-                r.mean = c + D / n;
-                r.m2 = fmax(Q - D * (D / n), 0.0);
-                r.itm = itm;
-            }
-            out[static_cast<int64_t>(blockIdx.x) * QK_MAX_PAYOFFS + k] = r;
-        }
+        const Moments r = merge_range(partials + t.partial_base + k, t.n_tiles, np, red);
+        if (threadIdx.x == 0) out[static_cast<int64_t>(blockIdx.x) * QK_MAX_PAYOFFS + k] = r;
+    }
+}
+
+// Two-level merge, level 1: one block per chunk of kMergeChunkTiles consecutive
+// tile records of one task, writing one record per chunk and leg
+// (chunks[chunk][QK_MAX_PAYOFFS]).  The chunk's task is found by binary search
+// over the tasks' chunk_base (ascending, every task has at least one chunk).
+__global__ void __launch_bounds__(256) merge_chunks_kernel(const TaskDev *__restrict__ tasks, int32_t n_tasks,
+                                                           const Moments *__restrict__ partials,
+                                                           Moments *__restrict__ chunks) {
+    __shared__ double red[4][32];
+    const int64_t b = blockIdx.x;
+    int lo = 0, hi = n_tasks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tasks[mid].chunk_base <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const TaskDev &t = tasks[lo];
+    const int np = t.n_payoffs;
+    const int64_t first = (b - t.chunk_base) * kMergeChunkTiles;
+    const int64_t count = min(static_cast<int64_t>(kMergeChunkTiles), static_cast<int64_t>(t.n_tiles) - first);
+    for (int k = 0; k < np; ++k) {
+        const Moments r = merge_range(partials + t.partial_base + first * np + k, count, np, red);
+        if (threadIdx.x == 0) chunks[b * QK_MAX_PAYOFFS + k] = r;
+    }
+}
+
+// Level 2: one block per task merges its chunk records.
+__global__ void __launch_bounds__(128) merge_task_chunks_kernel(const TaskDev *__restrict__ tasks,
+                                                                const Moments *__restrict__ chunks,
+                                                                TaskMoments *__restrict__ out) {
+    __shared__ double red[4][32];
+    const TaskDev &t = tasks[blockIdx.x];
+    for (int k = 0; k < t.n_payoffs; ++k) {
+        const Moments r = merge_range(chunks + t.chunk_base * QK_MAX_PAYOFFS + k, t.n_chunks, QK_MAX_PAYOFFS, red);
+        if (threadIdx.x == 0) out[static_cast<int64_t>(blockIdx.x) * QK_MAX_PAYOFFS + k] = r;
     }
 }
 
@@ -343,7 +484,7 @@ __global__ void __launch_bounds__(kPathBlock) slab_paths_kernel(const TaskDev *_
     if (i >= count) return;
     const TaskDev &t = *task;
     const StepConst<R> p = task_const<R>(t);
-    SlabSink<R> sink{slab_S, slab_v, ld, i, stride};
+    SlabSink<R> sink{slab_S, slab_v, ld, i, stride, stride};
     PathState<R> st;
     simulate_path<R, MODEL, SCHEME>(p, static_cast<R>(t.S0), static_cast<R>(t.v0), t.n_steps, ParamKeys{rk}, t.key0,
                                     t.key1, static_cast<uint32_t>(first_path + i), t.stream, t.jump_kmin, st, sink);
@@ -413,14 +554,15 @@ __global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double
 // ----------------------------------------------------------------------------
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
-                               unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed) {
+                               unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
+                               bool antithetic) {
     const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
                                                  static_cast<uint32_t>(seed >> 32));
     if (precision == QK_FP32)
-        price_kernel_for<float>(model, scheme, uniform_key)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<float>(model, scheme, uniform_key, antithetic)<<<grid, kPathBlock, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     else
-        price_kernel_for<double>(model, scheme, uniform_key)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<double>(model, scheme, uniform_key, antithetic)<<<grid, kPathBlock, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     return cudaGetLastError();
 }
@@ -430,6 +572,15 @@ cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks
     // one block per task; wide blocks only when some task has many tiles to read
     const int threads = max_tiles >= 4096 ? 1024 : 256;
     merge_tasks_kernel<<<n_tasks, threads, 0, s>>>(tasks, partials, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_two_level(int n_tasks, int64_t n_chunks, cudaStream_t s, const TaskDev *tasks,
+                                   const Moments *partials, Moments *chunks, TaskMoments *out) {
+    merge_chunks_kernel<<<static_cast<unsigned>(n_chunks), 256, 0, s>>>(tasks, n_tasks, partials, chunks);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    merge_task_chunks_kernel<<<n_tasks, 128, 0, s>>>(tasks, chunks, out);
     return cudaGetLastError();
 }
 
@@ -495,12 +646,14 @@ cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEven
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme) {
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, bool antithetic) {
     int nb = 0;
     if (precision == QK_FP32)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<float>(model, scheme), kPathBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<float>(model, scheme, true, antithetic),
+                                                      kPathBlock, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<double>(model, scheme), kPathBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<double>(model, scheme, true, antithetic),
+                                                      kPathBlock, 0);
     return nb > 0 ? nb : 1;
 }
 

@@ -98,6 +98,21 @@ class Handle:
         check(L.lib().qk_measure_sfu(self.ptr, C.byref(x)), "qk_measure_sfu")
         return x.value
 
+    def autotune(self, contracts: Sequence[L.Contract], greeks: L.Greeks | None = None, reps: int = 2) -> list[dict]:
+        """Time every launch shape per kernel kind on a sample and keep the fastest (qk_autotune)."""
+        n = len(contracts)
+        arr = (L.Contract * n)(*contracts)
+        rep = L.TuneReport()
+        check(L.lib().qk_autotune(self.ptr, arr, n, C.byref(greeks) if greeks else None, reps, C.byref(rep)),
+              "qk_autotune")
+        return [{"precision": rep.precision[k], "model": rep.model[k], "scheme": rep.scheme[k],
+                 "tiles_per_warp": rep.tiles_per_warp[k], "guided_tail": rep.guided_tail[k],
+                 "best_ms": rep.best_ms[k], "default_ms": rep.default_ms[k]} for k in range(rep.n_kinds)]
+
+    def tune_set(self, precision: int, model: int, scheme: int, tiles_per_warp: int, guided_tail: bool) -> None:
+        check(L.lib().qk_tune_set(self.ptr, precision, model, scheme, tiles_per_warp, int(guided_tail)),
+              "qk_tune_set")
+
 
 _default: Handle | None = None
 
@@ -117,7 +132,8 @@ def payoff(type: int = L.EUROPEAN, right: int = L.CALL, strike: float = 100.0, b
 def make_contract(*, S0=100.0, v0=0.04, r=0.03, q=0.0, model=L.HESTON, scheme=L.EULER, kappa=2.0, theta=0.04,
                   sigma=0.3, rho=-0.7, lambda_j=0.0, mu_j=0.0, sigma_j=0.0, psi_c=1.5, T=1.0, n_steps=252,
                   normalize=True, n_paths=100_000, seed=42, stream=0, precision=L.FP32,
-                  payoffs: Sequence[L.Payoff] | None = None, lsm_basis=L.LSM_LAGUERRE3, lsm_dates=0) -> L.Contract:
+                  payoffs: Sequence[L.Payoff] | None = None, lsm_basis=L.LSM_LAGUERRE3, lsm_dates=0,
+                  antithetic=False) -> L.Contract:
     c = L.Contract()
     c.S0, c.v0, c.r, c.q = S0, v0, r, q
     c.model, c.scheme = model, scheme
@@ -132,6 +148,7 @@ def make_contract(*, S0=100.0, v0=0.04, r=0.03, q=0.0, model=L.HESTON, scheme=L.
     for i, p in enumerate(legs):
         c.payoffs[i] = p
     c.lsm_basis, c.lsm_dates = lsm_basis, lsm_dates
+    c.antithetic = int(bool(antithetic))
     return c
 
 

@@ -293,7 +293,50 @@ def test_timing_and_launch_count(qk, handle):
     ks = [qk.make_contract(n_paths=100_000, seed=i + 1) for i in range(16)]
     qk.price_batch(ks, qk.make_greeks(qk.GREEK_ALL), handle)
     t = handle.last_timing()
-    assert t["launches"] == 2  # one persistent path kernel + one merge for 16 contracts x 12 tasks
+    assert t["launches"] == 3  # one persistent path kernel + the two-level merge for 16 contracts x 12 tasks
     assert t["device_ms"] > 0 and t["path_steps"] == pytest.approx(16 * 12 * 100_000 * 252)
     qk.price_plain(ks[0], qk.make_greeks(qk.GREEK_ALL), handle)
-    assert handle.last_timing()["launches"] == 12 + 1  # one FP64 launch per task, then the merge
+    assert handle.last_timing()["launches"] == 12 + 2  # one FP64 launch per task, then the two-level merge
+
+
+@pytest.mark.parametrize("model,scheme", [(0, 2), (1, 2), (1, 0)])
+def test_antithetic_pairs_match_oracle(qk, handle, oracle, model, scheme):
+    """Antithetic pairs (not in the reference): pair k shares path k's draws, its second member
+    with every normal negated; estimates over pair averages, against the oracle's pairs."""
+    base = dict(model=model, scheme=scheme, lambda_j=0.5 if model else 0.0, mu_j=-0.1, sigma_j=0.15, n_steps=48,
+                n_paths=20_000, seed=2024, payoffs=_legs(qk, ALL_LEGS[:8]), antithetic=True)
+    k = qk.make_contract(precision=qk.FP64, **base)
+    got = qk.price_plain(k, None, handle)["legs"]
+    want = oracle.price(k)["legs"]
+    for a, b in zip(got, want):
+        assert a["price"] == pytest.approx(b["price"], rel=1e-9, abs=1e-12), (a, b)
+        assert a["std_error"] == pytest.approx(b["std_error"], rel=1e-6, abs=1e-12)
+        assert a["prob_itm"] == pytest.approx(b["prob_itm"], rel=1e-9, abs=1e-12)
+    k32 = qk.make_contract(precision=qk.FP32, **base)
+    for a, b in zip(qk.price_batch([k32], None, handle)[0]["legs"], oracle.price(k32)["legs"]):
+        assert abs(a["price"] - b["price"]) <= 0.05 * b["std_error"] + 1e-7, (a, b)
+
+
+def test_antithetic_greeks_match_oracle(qk, handle, oracle):
+    g = qk.make_greeks(qk.GREEK_ALL, bump_S_rel=0.01, bump_vol=0.02, bump_r_abs=0.001, bump_T_abs=7 / 365)
+    k = qk.make_contract(scheme=qk.ANDERSEN_QE, n_steps=32, n_paths=20_000, seed=4242, precision=qk.FP64,
+                         payoffs=[qk.payoff(qk.ASIAN, qk.CALL, 100.0)], antithetic=True)
+    got = qk.price_batch([k], g, handle)[0]["legs"][0]
+    want = oracle.price(k, g)["legs"][0]
+    for f in ("price", "delta", "gamma", "vega", "vomma", "vanna", "rho", "theta"):
+        assert got[f] == pytest.approx(want[f], rel=1e-7, abs=1e-9), f
+
+
+def test_antithetic_reduces_error_and_validates(qk, handle, oracle):
+    base = dict(scheme=qk.ANDERSEN_QE, n_steps=64, n_paths=400_000, seed=99, precision=qk.FP32,
+                payoffs=[qk.payoff(qk.EUROPEAN, qk.CALL, 100.0)])
+    plain = qk.price_batch([qk.make_contract(**base)], None, handle)[0]["legs"][0]
+    anti = qk.price_batch([qk.make_contract(antithetic=True, **base)], None, handle)[0]["legs"][0]
+    assert anti["std_error"] < 0.8 * plain["std_error"]
+    exact = oracle.exact_call(1, qk.make_contract(**base), 200.0)
+    assert abs(anti["price"] - exact) <= 3.0 * anti["std_error"] + 5e-3
+    with pytest.raises(ValueError, match="even"):
+        qk.price_batch([qk.make_contract(antithetic=True, **{**base, "n_paths": 1001})], None, handle)
+    with pytest.raises(RuntimeError, match="antithetic"):
+        qk.price_batch([qk.make_contract(antithetic=True, **{**base, "payoffs": [qk.payoff(qk.AMERICAN, qk.PUT, 100.0)]})],
+                       None, handle)

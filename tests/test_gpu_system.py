@@ -231,3 +231,28 @@ def test_prepared_batch_graph_replay(qk, handle):
     qk.price_batch(batch[:1], None, handle)
     with pytest.raises(RuntimeError, match="qk_batch_prepare"):
         prep.run()
+
+
+def test_autotuner_keeps_prices_and_reports_every_kind(qk, handle):
+    """The autotuner times every candidate shape per kernel kind and keeps the fastest; a shape
+    changes which paths share a tile record, never which paths are simulated, so prices agree to
+    the rounding of the moment merge."""
+    from quantkos_b200 import workloads as W
+    batch = [c for c in W.mixed_batch(48, seed=9)]
+    for c in batch:
+        c.n_paths = min(c.n_paths, 200_000)
+    before = qk.price_batch(batch, None, handle)
+    report = handle.autotune(batch, None, reps=1)
+    kinds = {(c.precision, c.model, c.scheme) for c in batch}
+    assert {(r["precision"], r["model"], r["scheme"]) for r in report} == kinds
+    for r in report:
+        assert r["tiles_per_warp"] in (4, 8, 12, 24, 48) and r["guided_tail"] in (0, 1)
+        assert 0.0 < r["best_ms"] <= r["default_ms"]
+    after = qk.price_batch(batch, None, handle)
+    for a, b in zip(before, after):
+        assert a["legs"][0]["price"] == pytest.approx(b["legs"][0]["price"], rel=1e-12, abs=1e-15)
+        assert a["legs"][0]["std_error"] == pytest.approx(b["legs"][0]["std_error"], rel=1e-9)
+    with pytest.raises(ValueError):
+        handle.tune_set(1, 0, 3, 12, True)
+    for r in report:  # back to the defaults for the tests that follow
+        handle.tune_set(r["precision"], r["model"], r["scheme"], 24, False)
