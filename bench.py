@@ -201,9 +201,12 @@ def _timed(torch, ext, fn, steps: int, flush=None) -> list[float]:
 
 
 def run_other_workload(args) -> None:
+    import ctypes as C
+
     import torch
 
     import quantkos_b200 as qk
+    from quantkos_b200 import _lib as L
     from quantkos_b200 import workloads as W
 
     torch.cuda.set_device(0)
@@ -317,13 +320,37 @@ def run_other_workload(args) -> None:
         st = srv.stats()
         srv.stop()
         offered = W.path_steps(contracts)
+        # the plain FP64 one-contract-per-launch method on a sample of the same requests
+        sample = contracts[:args.subset]
+        sample64 = []
+        for c in sample:
+            c64 = L.Contract()
+            C.memmove(C.byref(c64), C.byref(c), C.sizeof(L.Contract))
+            c64.precision = qk.FP64
+            sample64.append(c64)
+        qk.price_plain(sample64[0], None, h)
+        plain_res = []
+
+        def plain_all():
+            plain_res.clear()
+            for c in sample64:
+                plain_res.append(qk.price_plain(c, None, h))
+
+        t_plain = _timed(torch, ext, plain_all, 1, flush)[0]
+        batch_res = qk.price_batch(sample, None, h)
+        t_batch = _timed(torch, ext, lambda: qk.price_batch(sample, None, h), 1, flush)[0]
+        se_ratio = statistics.mean(a["legs"][0]["std_error"] / b["legs"][0]["std_error"]
+                                   for a, b in zip(batch_res, plain_res) if b["legs"][0]["std_error"] > 0)
         line.update(metric="contracts/s", unit="contracts/s", value=st["contracts_per_s"], dtype="f32",
                     ms_per_step=None,
                     config={"workload": f"serving_{args.requests}_requests_poisson_2000_per_s_30pct_american",
                             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"],
                             "max_ms": st["max_ms"], "path_steps_per_s": st["path_steps_per_s"],
                             "offered_path_steps": offered, "offered_path_steps_per_s": offered / arrivals[-1],
-                            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"]},
+                            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
+                            "sample": len(sample), "sample_plain_fp64_contracts_per_s": len(sample) / (t_plain * 1e-3),
+                            "sample_batched_contracts_per_s": len(sample) / (t_batch * 1e-3),
+                            "sample_mean_se_ratio_batched_over_plain": se_ratio},
                     gpu_launches=None)
     pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     line["clocks"] = sampler.summary(pk.get("sm_max_mhz", 1965.0))
@@ -375,6 +402,7 @@ def main() -> None:
     if not args.no_autotune:
         rep = h.autotune([contract], None, reps=1)[0]
         tuned = {"tiles_per_warp": rep["tiles_per_warp"], "guided_tail": rep["guided_tail"],
+                 "paths_per_lane": rep["paths_per_lane"],
                  "best_ms": rep["best_ms"], "default_ms": rep["default_ms"]}
 
     # ---- value: descriptors resident in HBM, K device-timed pricings

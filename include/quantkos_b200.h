@@ -197,10 +197,11 @@ qk_status qk_batch_fetch(qk_handle *h, qk_result *out, int32_t n);
 /* ---------------------------------------------------------------- autotuner
  * Launch shape of the batched engine, per kernel kind (precision x model x
  * scheme): the target number of warp tiles per resident warp slot (sets the
- * paths per tile) and whether a task that fills the GPU many times over ends in
- * short "tail" tiles.  The reference sizes its path batches from a memory budget
+ * paths per tile), whether a task that fills the GPU many times over ends in
+ * short "tail" tiles, and whether a lane simulates one path or two independent
+ * paths (2u, 2u+1) interleaved.  The reference sizes its path batches from a memory budget
  * (include/core/memory/PathsMCBatchMem.hpp:330-420); there it has no tuner.
- * Defaults: 24 tiles per warp slot, guided tail off. */
+ * Defaults: 24 tiles per warp slot, guided tail off, one path per lane. */
 #define QK_TUNE_KINDS 12
 typedef struct qk_tune_report {
     int32_t n_kinds;                         /* kinds present in the sample */
@@ -209,6 +210,7 @@ typedef struct qk_tune_report {
     int32_t scheme[QK_TUNE_KINDS];
     int32_t tiles_per_warp[QK_TUNE_KINDS];   /* chosen */
     int32_t guided_tail[QK_TUNE_KINDS];      /* chosen: 1 = on */
+    int32_t paths_per_lane[QK_TUNE_KINDS];   /* chosen: 1 or 2 */
     double best_ms[QK_TUNE_KINDS];           /* device time of pricing the sample's tasks of this kind, chosen shape */
     double default_ms[QK_TUNE_KINDS];        /* the same with the defaults */
     int32_t candidates;                      /* shapes timed per kind */
@@ -216,14 +218,14 @@ typedef struct qk_tune_report {
 
 /* Times the sample `c` (forward contracts; American ones are skipped) kind by
  * kind under every candidate shape (tiles per warp slot 4, 8, 12, 24, 48; tail
- * off, on), `reps` timed runs each after one warm-up, keeps the fastest shape per kind
+ * off, on; 1 or 2 paths per lane), `reps` timed runs each after one warm-up, keeps the fastest shape per kind
  * in the handle for later qk_price_batch / qk_batch_prepare calls and reports it.
  * Prices do not depend on the shape beyond the last bits of the moment merge. */
 qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g, int32_t reps,
                       qk_tune_report *out);
 /* Sets one kind's shape by hand (for example a stored autotuner result). */
 qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t scheme, int32_t tiles_per_warp,
-                      int32_t guided_tail);
+                      int32_t guided_tail, int32_t paths_per_lane);
 
 /* qk_price_noalloc — no counterpart in the reference.  The base price (no Greeks)
  * of one forward contract for callers that cannot allocate device memory on the

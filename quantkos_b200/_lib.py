@@ -84,7 +84,8 @@ TUNE_KINDS = 12
 class TuneReport(C.Structure):
     _fields_ = [("n_kinds", C.c_int32), ("precision", C.c_int32 * TUNE_KINDS), ("model", C.c_int32 * TUNE_KINDS),
                 ("scheme", C.c_int32 * TUNE_KINDS), ("tiles_per_warp", C.c_int32 * TUNE_KINDS),
-                ("guided_tail", C.c_int32 * TUNE_KINDS), ("best_ms", C.c_double * TUNE_KINDS),
+                ("guided_tail", C.c_int32 * TUNE_KINDS), ("paths_per_lane", C.c_int32 * TUNE_KINDS),
+                ("best_ms", C.c_double * TUNE_KINDS),
                 ("default_ms", C.c_double * TUNE_KINDS), ("candidates", C.c_int32)]
 
 
@@ -128,7 +129,7 @@ SIGNATURES = {
     "qk_get_stream": (C.c_int, [_VP, _P(_VP)]),
     "qk_last_timing": (C.c_int, [_VP, _P(Timing)]),
     "qk_autotune": (C.c_int, [_VP, _P(Contract), C.c_int32, _P(Greeks), C.c_int32, _P(TuneReport)]),
-    "qk_tune_set": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "qk_tune_set": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "qk_measure_sfu": (C.c_int, [_VP, _P(C.c_double)]),
     "qk_validate": (C.c_int, [_P(Contract), _P(Greeks)]),
     "qk_price_plain": (C.c_int, [_VP, _P(Contract), _P(Greeks), _P(Result)]),

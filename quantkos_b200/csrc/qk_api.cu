@@ -195,7 +195,7 @@ std::vector<int> roles_for(const qk_greeks *g, double T) {
     return roles;
 }
 
-TaskDev make_task(const qk_contract &b, int ppt) {
+TaskDev make_task(const qk_contract &b, int ppt, int lane_mode) {
     TaskDev t;
     std::memset(&t, 0, sizeof(t));
     const double dt = b.T / b.n_steps;
@@ -217,8 +217,8 @@ TaskDev make_task(const qk_contract &b, int ppt) {
     const float Lf = t.cf.exp_m_lambda_dt;
     const double kd = std::ceil(static_cast<double>(Lf) * 8388608.0 - 0.5);
     t.jump_kmin = static_cast<uint32_t>(std::min(std::max(kd, 0.0), 8388608.0));
-    t.antithetic = b.antithetic ? 1 : 0;
-    const int64_t units = t.antithetic ? b.n_paths / 2 : b.n_paths;  // a lane simulates a path or a pair
+    t.lane_mode = b.antithetic ? kLanePair : lane_mode;
+    const int64_t units = lane_units(b.n_paths, t.lane_mode);
     const int64_t tile_units = static_cast<int64_t>(kWarpTilePaths) * ppt;
     t.n_tiles = static_cast<int32_t>((units + tile_units - 1) / tile_units);
     t.n_big = t.n_tiles;  // uniform tiles unless split_tail is applied
@@ -238,7 +238,7 @@ TaskDev make_task(const qk_contract &b, int ppt) {
 // take short tail tiles, so all warps end within a short tile of each other; the
 // record count stays below that of uniform ppt-round tiles.
 static void split_tail(TaskDev &t, int64_t warp_slots) {
-    const int64_t units = t.antithetic ? t.n_paths / 2 : t.n_paths;
+    const int64_t units = lane_units(t.n_paths, t.lane_mode);
     const int64_t rounds = (units + kWarpTilePaths - 1) / kWarpTilePaths;
     if (t.ppt < 4 || rounds < 4 * warp_slots * static_cast<int64_t>(t.ppt)) return;
     const int big = 2 * t.ppt;
@@ -258,7 +258,8 @@ static double step_cost(const TaskDev &t) {
     if (t.scheme == QK_ANDERSEN_QE) c *= 1.6;
     if (t.model == QK_BATES) c *= 1.25;
     if (t.precision == QK_FP64) c *= 6.0;
-    if (t.antithetic) c *= 1.7;  // two paths per lane, one set of draws
+    if (t.lane_mode == kLanePair) c *= 1.7;  // two paths per lane, one set of draws
+    if (t.lane_mode == kLaneTwo) c *= 2.0;
     return c;
 }
 
@@ -325,7 +326,12 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     plan.status.assign(n, QK_OK);
     plan.task_of.assign(static_cast<size_t>(n) * kNumRoles, -1);
     // paths per kernel kind (precision, model, scheme): each kind is one launch
-    int64_t kind_paths[2][2][3][2] = {};  // [precision][model][scheme][antithetic]: lanes' units per launch
+    int64_t kind_paths[2][2][3][3] = {};  // [precision][model][scheme][lane mode]: lane units per launch
+    auto lane_mode_of = [&](const qk_contract &c, int pr) {
+        if (c.antithetic) return static_cast<int>(kLanePair);
+        if (plain) return static_cast<int>(kLaneOne);
+        return h->tune_lanes[pr][c.model][c.scheme] == 2 ? static_cast<int>(kLaneTwo) : static_cast<int>(kLaneOne);
+    };
     for (int i = 0; i < n; ++i) {
         const qk_greeks *g = plan.g_of(i);
         const qk_status s = validate_contract(cs[i], g);
@@ -337,9 +343,9 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
             continue;
         }
         const int pr = plain ? QK_FP64 : cs[i].precision;
-        const int64_t units = cs[i].antithetic ? cs[i].n_paths / 2 : cs[i].n_paths;
-        kind_paths[pr][cs[i].model][cs[i].scheme][cs[i].antithetic ? 1 : 0] +=
-            units * static_cast<int64_t>(roles_for(g, cs[i].T).size());
+        const int lm = lane_mode_of(cs[i], pr);
+        kind_paths[pr][cs[i].model][cs[i].scheme][lm] +=
+            lane_units(cs[i].n_paths, lm) * static_cast<int64_t>(roles_for(g, cs[i].T).size());
     }
     struct Item {
         TaskDev t;
@@ -350,19 +356,19 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     for (int i = 0; i < n; ++i) {
         if (cs[i].payoffs[0].type == QK_AMERICAN) continue;
         const int pr = plain ? QK_FP64 : cs[i].precision;
-        const bool anti = cs[i].antithetic != 0;
-        const int64_t units = anti ? cs[i].n_paths / 2 : cs[i].n_paths;
-        const int64_t launch_units = plain ? units : kind_paths[pr][cs[i].model][cs[i].scheme][anti ? 1 : 0];
+        const int lm = lane_mode_of(cs[i], pr);
+        const int64_t units = lane_units(cs[i].n_paths, lm);
+        const int64_t launch_units = plain ? units : kind_paths[pr][cs[i].model][cs[i].scheme][lm];
         const int ppt = choose_ppt(units, launch_units, h->sm_count,
                                    plain ? kPlainTilesPerWarp : h->tune_tpw[pr][cs[i].model][cs[i].scheme]);
         const bool tail = !plain && h->tune_tail[pr][cs[i].model][cs[i].scheme];
         const int64_t warp_slots = static_cast<int64_t>(h->sm_count) *
-                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, anti) *
+                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, lm) *
                                    (kPathBlock / 32);
         const qk_greeks *g = plan.g_of(i);
         for (int role : roles_for(g, cs[i].T)) {
             const qk_contract b = bumped(plan.norm[i], g, role);
-            Item it{make_task(b, ppt), i, role, 0.0};
+            Item it{make_task(b, ppt, lm), i, role, 0.0};
             if (tail) split_tail(it.t, warp_slots);
             it.cost = step_cost(it.t) * b.n_steps * b.n_payoffs * 0.02 + step_cost(it.t) * b.n_steps;
             items.push_back(it);
@@ -372,7 +378,7 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         // group by kernel (precision, model, scheme); longest tiles first inside a group
         std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
             if (a.t.precision != b.t.precision) return a.t.precision < b.t.precision;
-            if (a.t.antithetic != b.t.antithetic) return a.t.antithetic < b.t.antithetic;
+            if (a.t.lane_mode != b.t.lane_mode) return a.t.lane_mode < b.t.lane_mode;
             if (a.t.model != b.t.model) return a.t.model < b.t.model;
             if (a.t.scheme != b.t.scheme) return a.t.scheme < b.t.scheme;
             return a.cost > b.cost;
@@ -441,13 +447,13 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
     if (plan.plain) {
         for (size_t i = 0; i < nt; ++i) {
             const TaskDev &t = plan.tasks[i];
-            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme, t.antithetic != 0);
+            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme, t.lane_mode);
             const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
             // one task: its own queue cursor, its own tile range (prefix of one task = itself)
             const uint64_t seed = static_cast<uint64_t>(t.key0) | (static_cast<uint64_t>(t.key1) << 32);
             QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
                                            t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed,
-                                           t.antithetic != 0));
+                                           t.lane_mode));
             h->launches++;
         }
     } else {
@@ -456,11 +462,11 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             size_t e = b;
             const TaskDev &tb = plan.tasks[b];
             while (e < nt && plan.tasks[e].precision == tb.precision && plan.tasks[e].model == tb.model &&
-                   plan.tasks[e].scheme == tb.scheme && plan.tasks[e].antithetic == tb.antithetic)
+                   plan.tasks[e].scheme == tb.scheme && plan.tasks[e].lane_mode == tb.lane_mode)
                 ++e;
             const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
             const int64_t slots = slots_end - tb.tile_begin;
-            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.antithetic != 0);
+            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.lane_mode);
             const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
             bool uniform_key = true;
             for (size_t i = b; i < e; ++i)
@@ -468,7 +474,7 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
             QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
                                            static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
-                                           uniform_key, seed, tb.antithetic != 0));
+                                           uniform_key, seed, tb.lane_mode));
             h->launches++;
             b = e;
         }

@@ -76,6 +76,7 @@ struct qk_handle {
     // launch shape per kernel kind [precision][model][scheme] (autotuner)
     int tune_tpw[2][2][3] = {{{24, 24, 24}, {24, 24, 24}}, {{24, 24, 24}, {24, 24, 24}}};
     int tune_tail[2][2][3] = {};
+    int tune_lanes[2][2][3] = {{{1, 1, 1}, {1, 1, 1}}, {{1, 1, 1}, {1, 1, 1}}};  // paths per lane: 1 or 2
     qk_timing timing{};
     int64_t launches = 0;
     int64_t h2d_bytes = 0, d2h_bytes = 0;
@@ -89,7 +90,7 @@ namespace qk {
 
 enum : int { kNumRoles = 12 };
 
-TaskDev make_task(const qk_contract &b, int ppt);
+TaskDev make_task(const qk_contract &b, int ppt, int lane_mode = kLaneOne);
 qk_contract normalised(const qk_contract &c, double *scale);
 qk_contract bumped(const qk_contract &n, const qk_greeks *g, int role);
 std::vector<int> roles_for(const qk_greeks *g, double T);

@@ -58,6 +58,15 @@ struct PayoffSpec {
 };
 
 // One pricing task on the device: a contract, or one of its Greek bumps.
+// What one lane of the path kernel simulates: one path; an antithetic pair
+// (paths 2u and 2u+1 from pair u's draws, the second negated); or two independent
+// consecutive paths 2u and 2u+1 (instruction-level parallelism).
+enum : int { kLaneOne = 0, kLanePair = 1, kLaneTwo = 2 };
+
+__host__ __device__ inline int64_t lane_units(int64_t n_paths, int lane_mode) {
+    return lane_mode == kLaneOne ? n_paths : (lane_mode == kLanePair ? n_paths / 2 : (n_paths + 1) / 2);
+}
+
 struct TaskDev {
     StepConst<float> cf;
     StepConst<double> cd;
@@ -76,7 +85,7 @@ struct TaskDev {
     int32_t ppt_tail;
     int64_t chunk_base;    // first merge chunk of the task (two-level merge of the tile records)
     int32_t n_chunks;      // merge chunks of the task: ceil(n_tiles / kMergeChunkTiles)
-    int32_t antithetic;    // 1: a lane simulates pair u (paths 2u, 2u+1); tiles count pairs
+    int32_t lane_mode;     // kLaneOne / kLanePair / kLaneTwo: what a lane simulates; tiles count lane units
     PayoffSpec pay[QK_MAX_PAYOFFS];
 };
 

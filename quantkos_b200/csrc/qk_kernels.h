@@ -16,11 +16,11 @@ constexpr int kPathMinBlocksFp32 = QK_PATH_MIN_BLOCKS_FP32;  // resident blocks 
 
 // uniform_key: every task of the launch has Philox key `seed` (round keys go in the
 // kernel parameters); otherwise each task's key is read from its descriptor.
-// antithetic: every task of the launch samples antithetic pairs.
+// lane_mode: what a lane simulates for every task of the launch (TaskDev::lane_mode).
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
                                unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
-                               bool antithetic = false);
+                               int lane_mode = kLaneOne);
 // max_tiles: the largest n_tiles among the tasks (sets the block width).
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
                                TaskMoments *out, int64_t max_tiles = 0);
@@ -36,7 +36,7 @@ cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t see
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
                               int umax, int n, double *S_out, double *v_out, int *status);
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, bool antithetic = false);
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode = kLaneOne);
 // Times a kernel of independent ex2.approx chains; returns its duration and MUFU op count.
 cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
                              double *ops);

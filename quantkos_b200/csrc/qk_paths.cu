@@ -135,30 +135,54 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
     }
 }
 
-// Antithetic pair: one set of draws, the second path with every normal negated.
-template <class R, int MODEL, int SCHEME>
-__device__ __forceinline__ void one_step_pair(const StepConst<R> &p, PathState<R> &a, PathState<R> &b, uint32_t wa,
-                                              uint32_t wb, uint32_t wpois, uint32_t kmin, uint32_t k0, uint32_t k1,
-                                              uint32_t path, uint32_t stream, int n) {
-    R z1, z2;
-    Math<R>::box_muller(wa, wb, z1, z2);
-    heston_step<R, SCHEME>(p, a.S, a.v, z1, z2);
-    heston_step<R, SCHEME>(p, b.S, b.v, -z1, -z2);
+// Two paths per lane.  NEG: an antithetic pair — one set of draws (those of path
+// a), path b with every normal negated and the same Poisson uniforms.  Otherwise
+// two independent paths, each with its own draws, interleaved for instruction-level
+// parallelism.
+template <class R, int MODEL, int SCHEME, bool NEG>
+__device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R> &a, PathState<R> &b, uint32_t wa1,
+                                             uint32_t wa2, uint32_t wb1, uint32_t wb2, uint32_t pois_a,
+                                             uint32_t pois_b, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path_a,
+                                             uint32_t path_b, uint32_t stream, int n) {
+    R za1, za2;
+    Math<R>::box_muller(wa1, wa2, za1, za2);
+    heston_step<R, SCHEME>(p, a.S, a.v, za1, za2);
+    if constexpr (NEG) {
+        heston_step<R, SCHEME>(p, b.S, b.v, -za1, -za2);
+    } else {
+        R zb1, zb2;
+        Math<R>::box_muller(wb1, wb2, zb1, zb2);
+        heston_step<R, SCHEME>(p, b.S, b.v, zb1, zb2);
+    }
     if constexpr (MODEL == kBates) {
-        if (jump_test<R>(wpois, p, kmin)) {
-            PhiloxJumpDraws<R> d{k0, k1, path, stream, static_cast<uint32_t>(n), Math<R>::u01(wpois), 1, 0, U4{0, 0, 0, 0}};
-            R fa, fb;
-            jump_factor_pair<R>(p, d.first, d, fa, fb);
-            a.S *= fa;
-            b.S *= fb;
+        if constexpr (NEG) {
+            if (jump_test<R>(pois_a, p, kmin)) {
+                PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(pois_a), 1, 0,
+                                     U4{0, 0, 0, 0}};
+                R fa, fb;
+                jump_factor_pair<R>(p, d.first, d, fa, fb);
+                a.S *= fa;
+                b.S *= fb;
+            }
+        } else {
+            if (jump_test<R>(pois_a, p, kmin)) {
+                PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(pois_a), 1, 0,
+                                     U4{0, 0, 0, 0}};
+                a.S *= jump_factor<R>(p, d.first, d);
+            }
+            if (jump_test<R>(pois_b, p, kmin)) {
+                PhiloxJumpDraws<R> d{k0, k1, path_b, stream, static_cast<uint32_t>(n), Math<R>::u01(pois_b), 1, 0,
+                                     U4{0, 0, 0, 0}};
+                b.S *= jump_factor<R>(p, d.first, d);
+            }
         }
     }
 }
 
-template <class R, int MODEL, int SCHEME, class Gen>
-__device__ __forceinline__ void simulate_pair(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
-                                              uint32_t k0, uint32_t k1, uint32_t pair, uint32_t stream, uint32_t kmin,
-                                              PathState<R> &a, PathState<R> &b) {
+template <class R, int MODEL, int SCHEME, bool NEG, class Gen>
+__device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
+                                             uint32_t k0, uint32_t k1, uint32_t path_a, uint32_t path_b,
+                                             uint32_t stream, uint32_t kmin, PathState<R> &a, PathState<R> &b) {
     a.S = b.S = S0;
     a.v = b.v = v0;
     a.ssum = b.ssum = 0.0;
@@ -167,28 +191,41 @@ __device__ __forceinline__ void simulate_pair(const StepConst<R> &p, R S0, R v0,
     for (int n0 = 0; n0 < n_steps; n0 += kSumChunk) {
         const int n1 = min(n0 + kSumChunk, n_steps);
         R blk_a = R(0), blk_b = R(0);
-        U4 wp{0u, 0u, 0u, 0u};
+        U4 pa{0u, 0u, 0u, 0u}, pb{0u, 0u, 0u, 0u};
         int n = n0;
         for (; n + 1 < n1; n += 2) {
-            const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), pair, stream, 0u});
+            const U4 wa = gen(U4{static_cast<uint32_t>(n >> 1), path_a, stream, 0u});
+            U4 wb{0u, 0u, 0u, 0u};
+            if constexpr (!NEG) wb = gen(U4{static_cast<uint32_t>(n >> 1), path_b, stream, 0u});
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), pair, stream, 2u});
+                if ((n & 3) == 0) {
+                    pa = gen(U4{static_cast<uint32_t>(n >> 2), path_a, stream, 2u});
+                    if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
+                }
             }
             const bool lo = (n & 3) == 0;
-            one_step_pair<R, MODEL, SCHEME>(p, a, b, w.x, w.y, lo ? wp.x : wp.z, kmin, k0, k1, pair, stream, n);
+            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, lo ? pa.x : pa.z, lo ? pb.x : pb.z,
+                                                kmin, k0, k1, path_a, path_b, stream, n);
             track(a, blk_a);
             track(b, blk_b);
-            one_step_pair<R, MODEL, SCHEME>(p, a, b, w.z, w.w, lo ? wp.y : wp.w, kmin, k0, k1, pair, stream, n + 1);
+            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.z, wa.w, wb.z, wb.w, lo ? pa.y : pa.w, lo ? pb.y : pb.w,
+                                                kmin, k0, k1, path_a, path_b, stream, n + 1);
             track(a, blk_a);
             track(b, blk_b);
         }
         if (n < n1) {
-            const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), pair, stream, 0u});
+            const U4 wa = gen(U4{static_cast<uint32_t>(n >> 1), path_a, stream, 0u});
+            U4 wb{0u, 0u, 0u, 0u};
+            if constexpr (!NEG) wb = gen(U4{static_cast<uint32_t>(n >> 1), path_b, stream, 0u});
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), pair, stream, 2u});
+                if ((n & 3) == 0) {
+                    pa = gen(U4{static_cast<uint32_t>(n >> 2), path_a, stream, 2u});
+                    if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
+                }
             }
-            one_step_pair<R, MODEL, SCHEME>(p, a, b, w.x, w.y, (n & 3) == 0 ? wp.x : wp.z, kmin, k0, k1, pair, stream,
-                                            n);
+            const bool lo = (n & 3) == 0;
+            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, lo ? pa.x : pa.z, lo ? pb.x : pb.z,
+                                                kmin, k0, k1, path_a, path_b, stream, n);
             track(a, blk_a);
             track(b, blk_b);
         }
@@ -240,7 +277,9 @@ __device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int
     return lo;
 }
 
-template <class R, int MODEL, int SCHEME, bool UK, bool ANTI>
+// LANE: kLaneOne (a lane simulates one path), kLanePair (an antithetic pair),
+// kLaneTwo (two independent paths 2u and 2u+1).
+template <class R, int MODEL, int SCHEME, bool UK, int LANE>
 __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp32 : 1)
     price_tiles_kernel(const TaskDev *__restrict__ tasks, const int64_t *__restrict__ prefix, int32_t n_tasks,
                        int64_t slot_begin, int64_t slot_end, unsigned long long *__restrict__ cursor,
@@ -278,23 +317,27 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
         if (lane < np) acc[lane] = Moments{0.0, 0.0, 0.0, 0.0};
         __syncwarp();
 
-        // a lane's unit is one path, or one antithetic pair of paths
-        const int64_t n_units = ANTI ? (n_paths >> 1) : n_paths;
+        // a lane's unit: one path, one antithetic pair, or two consecutive paths
+        const int64_t n_units = lane_units(n_paths, LANE);
         const int64_t left = n_units - tile_first;
         const int rounds =
             static_cast<int>(min(static_cast<int64_t>(tile_rounds), (left + kWarpTilePaths - 1) / kWarpTilePaths));
         for (int j = 0; j < rounds; ++j) {
             const int64_t unit = tile_first + static_cast<int64_t>(j) * kWarpTilePaths + lane;
             const bool active = unit < n_units;
-            if constexpr (ANTI) {
+            if constexpr (LANE != kLaneOne) {
+                constexpr bool NEG = LANE == kLanePair;
+                const uint32_t pa = NEG ? static_cast<uint32_t>(unit) : static_cast<uint32_t>(2 * unit);
+                const uint32_t pb = NEG ? pa : pa + 1u;
+                const bool active_b = NEG ? active : (active && static_cast<int64_t>(pb) < n_paths);
                 PathState<R> sa, sb;
                 if (active) {
                     if constexpr (UK) {
-                        simulate_pair<R, MODEL, SCHEME>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
-                                                        static_cast<uint32_t>(unit), stream, kmin, sa, sb);
+                        simulate_two<R, MODEL, SCHEME, NEG>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1, pa, pb, stream,
+                                                            kmin, sa, sb);
                     } else {
-                        simulate_pair<R, MODEL, SCHEME>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
-                                                        static_cast<uint32_t>(unit), stream, kmin, sa, sb);
+                        simulate_two<R, MODEL, SCHEME, NEG>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1, pa, pb,
+                                                            stream, kmin, sa, sb);
                     }
                 } else {
                     sa.S = sa.smax = sa.smin = sb.S = sb.smax = sb.smin = R(0);
@@ -303,9 +346,15 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
                 for (int k = 0; k < np; ++k) {
                     const PayoffSpec ps = t.pay[k];
                     const R xa = active ? final_payoff<R>(ps, sa.S, sa.ssum, sa.smax, sa.smin, n_steps) : R(0);
-                    const R xb = active ? final_payoff<R>(ps, sb.S, sb.ssum, sb.smax, sb.smin, n_steps) : R(0);
-                    const double y = 0.5 * (static_cast<double>(xa) + static_cast<double>(xb));
-                    const Moments wm = warp_moments_pair(y, active, xa > eps_payoff, xb > eps_payoff);
+                    const R xb = active_b ? final_payoff<R>(ps, sb.S, sb.ssum, sb.smax, sb.smin, n_steps) : R(0);
+                    Moments wm;
+                    if constexpr (NEG) {
+                        const double y = 0.5 * (static_cast<double>(xa) + static_cast<double>(xb));
+                        wm = warp_moments_pair(y, active, xa > eps_payoff, xb > eps_payoff);
+                    } else {
+                        wm = chan_merge(warp_moments(static_cast<double>(xa), active, xa > eps_payoff),
+                                        warp_moments(static_cast<double>(xb), active_b, xb > eps_payoff));
+                    }
                     if (lane == 0) acc[k] = chan_merge(acc[k], wm);
                 }
             } else {
@@ -340,25 +389,31 @@ template <class R>
 using PriceKernel = void (*)(const TaskDev *, const int64_t *, int32_t, int64_t, int64_t, unsigned long long *,
                              Moments *, const PhiloxRoundKeys);
 
-template <class R, bool UK, bool ANTI>
+template <class R, bool UK, int LANE>
 __host__ PriceKernel<R> price_kernel_for_keys(int model, int scheme) {
     switch (model * 3 + scheme) {
-        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK, ANTI>;
-        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK, ANTI>;
-        case 2: return price_tiles_kernel<R, kHeston, kQE, UK, ANTI>;
-        case 3: return price_tiles_kernel<R, kBates, kEuler, UK, ANTI>;
-        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK, ANTI>;
-        default: return price_tiles_kernel<R, kBates, kQE, UK, ANTI>;
+        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK, LANE>;
+        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK, LANE>;
+        case 2: return price_tiles_kernel<R, kHeston, kQE, UK, LANE>;
+        case 3: return price_tiles_kernel<R, kBates, kEuler, UK, LANE>;
+        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK, LANE>;
+        default: return price_tiles_kernel<R, kBates, kQE, UK, LANE>;
     }
 }
 
+template <class R, int LANE>
+__host__ PriceKernel<R> price_kernel_for_lane(int model, int scheme, bool uniform_key) {
+    return uniform_key ? price_kernel_for_keys<R, true, LANE>(model, scheme)
+                       : price_kernel_for_keys<R, false, LANE>(model, scheme);
+}
+
 template <class R>
-__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true, bool antithetic = false) {
-    if (antithetic)
-        return uniform_key ? price_kernel_for_keys<R, true, true>(model, scheme)
-                           : price_kernel_for_keys<R, false, true>(model, scheme);
-    return uniform_key ? price_kernel_for_keys<R, true, false>(model, scheme)
-                       : price_kernel_for_keys<R, false, false>(model, scheme);
+__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true, int lane_mode = kLaneOne) {
+    switch (lane_mode) {
+        case kLanePair: return price_kernel_for_lane<R, kLanePair>(model, scheme, uniform_key);
+        case kLaneTwo: return price_kernel_for_lane<R, kLaneTwo>(model, scheme, uniform_key);
+        default: return price_kernel_for_lane<R, kLaneOne>(model, scheme, uniform_key);
+    }
 }
 
 // Merging moment records.  A set of records (n_i, mean_i, M2_i, itm_i) is merged
@@ -555,14 +610,14 @@ __global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
                                unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
-                               bool antithetic) {
+                               int lane_mode) {
     const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
                                                  static_cast<uint32_t>(seed >> 32));
     if (precision == QK_FP32)
-        price_kernel_for<float>(model, scheme, uniform_key, antithetic)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<float>(model, scheme, uniform_key, lane_mode)<<<grid, kPathBlock, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     else
-        price_kernel_for<double>(model, scheme, uniform_key, antithetic)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<double>(model, scheme, uniform_key, lane_mode)<<<grid, kPathBlock, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     return cudaGetLastError();
 }
@@ -646,13 +701,13 @@ cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEven
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, bool antithetic) {
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode) {
     int nb = 0;
     if (precision == QK_FP32)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<float>(model, scheme, true, antithetic),
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<float>(model, scheme, true, lane_mode),
                                                       kPathBlock, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<double>(model, scheme, true, antithetic),
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<double>(model, scheme, true, lane_mode),
                                                       kPathBlock, 0);
     return nb > 0 ? nb : 1;
 }

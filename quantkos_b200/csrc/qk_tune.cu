@@ -3,7 +3,8 @@
 // The persistent path kernel balances its work through a device queue of warp
 // tiles; how many rounds a tile holds trades the queue's end-of-launch tail (big
 // tiles leave warps idle while the last ones finish) against per-tile overhead
-// (one FP64 record per tile and leg, merged afterwards).  The best point depends
+// (one FP64 record per tile and leg, merged afterwards), and a lane may carry two
+// independent paths (more instruction-level parallelism, twice the registers).  The best point depends
 // on the kernel kind and on the mix of contracts, so it is measured: the sample is
 // split by kind (precision, model, scheme), every kind is priced under each
 // candidate shape and the shortest device time of the call (CUDA events on the
@@ -26,20 +27,25 @@ namespace {
 
 constexpr int kTilesPerWarp[] = {4, 8, 12, 24, 48};
 constexpr int kTails[] = {0, 1};
+constexpr int kLanes[] = {1, 2};
 constexpr int kDefaultTpw = 24;  // the handle's defaults (qk_engine.h)
 constexpr int kDefaultTail = 0;
+constexpr int kDefaultLanes = 1;
 
 }  // namespace
 
 extern "C" qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t scheme,
-                                 int32_t tiles_per_warp, int32_t guided_tail) {
+                                 int32_t tiles_per_warp, int32_t guided_tail, int32_t paths_per_lane) {
     if (!h) return qk::fail(QK_ERR_INVALID_ARG, "qk_tune_set: NULL handle");
     if (precision < 0 || precision > 1 || model < 0 || model > 1 || scheme < 0 || scheme > 2)
         return qk::fail(QK_ERR_INVALID_ARG, "qk_tune_set: precision, model or scheme out of range");
     if (tiles_per_warp < 1 || tiles_per_warp > 1024)
         return qk::fail(QK_ERR_INVALID_ARG, "qk_tune_set: tiles_per_warp must be in [1, 1024]");
+    if (paths_per_lane != 1 && paths_per_lane != 2)
+        return qk::fail(QK_ERR_INVALID_ARG, "qk_tune_set: paths_per_lane must be 1 or 2");
     h->tune_tpw[precision][model][scheme] = tiles_per_warp;
     h->tune_tail[precision][model][scheme] = guided_tail ? 1 : 0;
+    h->tune_lanes[precision][model][scheme] = paths_per_lane;
     return QK_OK;
 }
 
@@ -48,7 +54,7 @@ extern "C" qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, 
     if (!h || !c || !out || n < 1) return qk::fail(QK_ERR_INVALID_ARG, "qk_autotune: NULL argument or empty sample");
     if (reps < 1 || reps > 100) return qk::fail(QK_ERR_INVALID_ARG, "qk_autotune: reps must be in [1, 100]");
     std::memset(out, 0, sizeof(*out));
-    out->candidates = static_cast<int32_t>(std::size(kTilesPerWarp) * std::size(kTails));
+    out->candidates = static_cast<int32_t>(std::size(kTilesPerWarp) * std::size(kTails) * std::size(kLanes));
     // sample indices per kind, forward contracts only
     std::vector<int> by_kind[QK_TUNE_KINDS];
     for (int i = 0; i < n; ++i) {
@@ -71,37 +77,43 @@ extern "C" qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, 
         }
         std::vector<qk_result> res(sub.size());
         double best = std::numeric_limits<double>::infinity(), dflt = 0.0;
-        int best_tpw = kDefaultTpw, best_tail = kDefaultTail;
-        for (int tpw : kTilesPerWarp)
-            for (int tail : kTails) {
-                h->tune_tpw[pr][md][sc] = tpw;
-                h->tune_tail[pr][md][sc] = tail;
-                double ms = std::numeric_limits<double>::infinity();
-                for (int r = 0; r <= reps; ++r) {  // run 0 warms up
-                    const qk_status s = qk::price_contracts(h, sub.data(), static_cast<int32_t>(sub.size()),
-                                                            gsub.data(), res.data(), false);
-                    if (s != QK_OK) {
-                        h->tune_tpw[pr][md][sc] = kDefaultTpw;
-                        h->tune_tail[pr][md][sc] = kDefaultTail;
-                        return s;
+        int best_tpw = kDefaultTpw, best_tail = kDefaultTail, best_lanes = kDefaultLanes;
+        for (int lanes : kLanes)
+            for (int tpw : kTilesPerWarp)
+                for (int tail : kTails) {
+                    h->tune_tpw[pr][md][sc] = tpw;
+                    h->tune_tail[pr][md][sc] = tail;
+                    h->tune_lanes[pr][md][sc] = lanes;
+                    double ms = std::numeric_limits<double>::infinity();
+                    for (int r = 0; r <= reps; ++r) {  // run 0 warms up
+                        const qk_status s = qk::price_contracts(h, sub.data(), static_cast<int32_t>(sub.size()),
+                                                                gsub.data(), res.data(), false);
+                        if (s != QK_OK) {
+                            h->tune_tpw[pr][md][sc] = kDefaultTpw;
+                            h->tune_tail[pr][md][sc] = kDefaultTail;
+                            h->tune_lanes[pr][md][sc] = kDefaultLanes;
+                            return s;
+                        }
+                        if (r > 0) ms = std::min(ms, h->timing.device_ms);
                     }
-                    if (r > 0) ms = std::min(ms, h->timing.device_ms);
+                    if (tpw == kDefaultTpw && tail == kDefaultTail && lanes == kDefaultLanes) dflt = ms;
+                    if (ms < best) {
+                        best = ms;
+                        best_tpw = tpw;
+                        best_tail = tail;
+                        best_lanes = lanes;
+                    }
                 }
-                if (tpw == kDefaultTpw && tail == kDefaultTail) dflt = ms;
-                if (ms < best) {
-                    best = ms;
-                    best_tpw = tpw;
-                    best_tail = tail;
-                }
-            }
         h->tune_tpw[pr][md][sc] = best_tpw;
         h->tune_tail[pr][md][sc] = best_tail;
+        h->tune_lanes[pr][md][sc] = best_lanes;
         const int k = out->n_kinds++;
         out->precision[k] = pr;
         out->model[k] = md;
         out->scheme[k] = sc;
         out->tiles_per_warp[k] = best_tpw;
         out->guided_tail[k] = best_tail;
+        out->paths_per_lane[k] = best_lanes;
         out->best_ms[k] = best;
         out->default_ms[k] = dflt;
     }

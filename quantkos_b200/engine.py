@@ -107,11 +107,13 @@ class Handle:
               "qk_autotune")
         return [{"precision": rep.precision[k], "model": rep.model[k], "scheme": rep.scheme[k],
                  "tiles_per_warp": rep.tiles_per_warp[k], "guided_tail": rep.guided_tail[k],
+                 "paths_per_lane": rep.paths_per_lane[k],
                  "best_ms": rep.best_ms[k], "default_ms": rep.default_ms[k]} for k in range(rep.n_kinds)]
 
-    def tune_set(self, precision: int, model: int, scheme: int, tiles_per_warp: int, guided_tail: bool) -> None:
-        check(L.lib().qk_tune_set(self.ptr, precision, model, scheme, tiles_per_warp, int(guided_tail)),
-              "qk_tune_set")
+    def tune_set(self, precision: int, model: int, scheme: int, tiles_per_warp: int, guided_tail: bool,
+                 paths_per_lane: int = 1) -> None:
+        check(L.lib().qk_tune_set(self.ptr, precision, model, scheme, tiles_per_warp, int(guided_tail),
+                                  paths_per_lane), "qk_tune_set")
 
 
 _default: Handle | None = None

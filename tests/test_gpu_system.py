@@ -247,6 +247,7 @@ def test_autotuner_keeps_prices_and_reports_every_kind(qk, handle):
     assert {(r["precision"], r["model"], r["scheme"]) for r in report} == kinds
     for r in report:
         assert r["tiles_per_warp"] in (4, 8, 12, 24, 48) and r["guided_tail"] in (0, 1)
+        assert r["paths_per_lane"] in (1, 2)
         assert 0.0 < r["best_ms"] <= r["default_ms"]
     after = qk.price_batch(batch, None, handle)
     for a, b in zip(before, after):
@@ -255,4 +256,4 @@ def test_autotuner_keeps_prices_and_reports_every_kind(qk, handle):
     with pytest.raises(ValueError):
         handle.tune_set(1, 0, 3, 12, True)
     for r in report:  # back to the defaults for the tests that follow
-        handle.tune_set(r["precision"], r["model"], r["scheme"], 24, False)
+        handle.tune_set(r["precision"], r["model"], r["scheme"], 24, False, 1)
