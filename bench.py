@@ -260,6 +260,8 @@ def run_other_workload(args) -> None:
         g = W.batch_greeks()
         full = W.mixed_batch()
         sub = full[:args.subset]
+        # launch shape per kernel kind from the autotuner on a sample of the batch (untimed)
+        tuned = [] if args.no_autotune else h.autotune(full[:256], g, reps=1)
         sub64 = W.mixed_batch(args.subset, precision=qk.FP64)
         qk.price_batch(sub, g, h)
         t_sub = _timed(torch, ext, lambda: qk.price_batch(sub, g, h), 1, flush)[0]
@@ -289,7 +291,9 @@ def run_other_workload(args) -> None:
                             "subset_plain_fp64_contracts_per_s": len(sub) / (t_plain * 1e-3),
                             "speedup_vs_plain_fp64_same_subset": t_plain / t_sub,
                             "mean_se_ratio_batched_over_plain": se_ratio,
-                            "subset_prices_within_3se_of_fp64": within},
+                            "subset_prices_within_3se_of_fp64": within,
+                            "autotune": [{k: r[k] for k in ("model", "scheme", "tiles_per_warp", "guided_tail",
+                                                            "paths_per_lane")} for r in tuned]},
                     gpu_launches=tf["launches"])
     else:  # serve
         arrivals, contracts = W.serving_stream(args.requests)

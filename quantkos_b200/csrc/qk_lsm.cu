@@ -259,13 +259,19 @@ __device__ int solve_scaled(const double *sums, double *c) {
         if (count > 0.0) c[0] = b[0] / count;
         return 2;
     }
-    for (int i = 0; i < NB; ++i) D[i] = G[i][i] > 0.0 ? sqrt(G[i][i]) : 1.0;
+    // one division per scale and per pivot (reciprocals), multiplications elsewhere:
+    // this runs on one thread between two dates, in the sweep's critical path
+    double invD[NB];
+    for (int i = 0; i < NB; ++i) {
+        D[i] = G[i][i] > 0.0 ? sqrt(G[i][i]) : 1.0;
+        invD[i] = 1.0 / D[i];
+    }
     for (int r = 0; r < NB; ++r) {
-        b[r] /= D[r];
-        for (int q = 0; q < NB; ++q) G[r][q] /= (D[r] * D[q]);
+        b[r] *= invD[r];
+        for (int q = 0; q < NB; ++q) G[r][q] *= invD[r] * invD[q];
     }
     // Cholesky
-    double L[NB][NB];
+    double L[NB][NB], invL[NB];
     bool ok = true;
     double lmin = 1e300, lmax = 0.0;
     for (int i = 0; i < NB && ok; ++i) {
@@ -278,10 +284,11 @@ __device__ int solve_scaled(const double *sums, double *c) {
                     break;
                 }
                 L[i][i] = sqrt(s);
+                invL[i] = 1.0 / L[i][i];
                 lmin = fmin(lmin, L[i][i]);
                 lmax = fmax(lmax, L[i][i]);
             } else {
-                L[i][jj] = s / L[jj][jj];
+                L[i][jj] = s * invL[jj];
             }
         }
     }
@@ -290,14 +297,14 @@ __device__ int solve_scaled(const double *sums, double *c) {
         for (int i = 0; i < NB; ++i) {
             double s = b[i];
             for (int k = 0; k < i; ++k) s -= L[i][k] * y[k];
-            y[i] = s / L[i][i];
+            y[i] = s * invL[i];
         }
         for (int i = NB - 1; i >= 0; --i) {
             double s = y[i];
             for (int k = i + 1; k < NB; ++k) s -= L[k][i] * c[k];
-            c[i] = s / L[i][i];
+            c[i] = s * invL[i];
         }
-        for (int i = 0; i < NB; ++i) c[i] /= D[i];
+        for (int i = 0; i < NB; ++i) c[i] *= invD[i];
         return 0;
     }
     // Householder QR with column pivoting on the scaled Gram (rank-revealing), then
@@ -390,6 +397,11 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, uint64_
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Programmatic dependent launch: the next date's kernel may start while this one
+// finishes; griddepcontrol.wait returns once the preceding grid has completed and
+// its writes are visible (immediately when there is no programmatic dependency).
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_preceding() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 constexpr int kLsmChunk = 4 * kLsmBlock;  // paths per staged chunk: four per thread
@@ -460,6 +472,7 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     extern __shared__ __align__(16) unsigned char lsm_smem[];
     R *stage = reinterpret_cast<R *>(lsm_smem);
 
+    pdl_launch_dependents();  // the next date's blocks may take SM slots as this grid drains
     const R K = static_cast<R>(a.K);
     const double inv_K = 1.0 / a.K;
     const R disc = static_cast<R>(a.disc);
@@ -467,13 +480,8 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     double acc[NACC];
 #pragma unroll
     for (int j = 0; j < NACC; ++j) acc[j] = 0.0;
-    double cu[NB];
-#pragma unroll
-    for (int i = 0; i < NB; ++i) cu[i] = 0.0;
     double cxu = 0.0, cvu = 0.0, cxg = 0.0, cvg = 0.0;
     if (!init) {
-#pragma unroll
-        for (int i = 0; i < NB; ++i) cu[i] = coeffs[d_upd * kMaxCoef + i];
         cxu = centre[2 * d_upd];
         cvu = centre[2 * d_upd + 1];
     }
@@ -490,30 +498,41 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     const int64_t n_chunks = (a.ld + kLsmChunk - 1) / kLsmChunk;
     constexpr int kPer16 = 16 / static_cast<int>(sizeof(R));  // elements per 16-byte copy
 
-    // Queue the copies of one chunk into stage st.  Rows hold ld elements, ld a
-    // multiple of 4, so no 16-byte group straddles the end of a row.
-    auto issue = [&](int64_t chunk, int st) {
+    // Queue the copies of one chunk into stage st: the slab rows (written by the
+    // forward kernel) and, unless `rows_only`, the cash flows (written by the
+    // previous date's launch).  Rows hold ld elements, ld a multiple of 4, so no
+    // 16-byte group straddles the end of a row.
+    auto issue = [&](int64_t chunk, int st, bool rows, bool flows) {
         R *base = stage + static_cast<size_t>(st) * L::kArrays * kLsmChunk;
         const int64_t p0 = chunk * kLsmChunk;
         for (int e = threadIdx.x * kPer16; e < kLsmChunk; e += kLsmBlock * kPer16) {
             const int64_t i = p0 + e;
             if (i >= a.ld) break;
-            cp_async16(base + L::kSu * kLsmChunk + e, Su + i, pol_first);
-            if (!init) cp_async16(base + L::kCf * kLsmChunk + e, cf + i, pol_last);
-            if (gram) cp_async16(base + L::kSg * kLsmChunk + e, Sg + i, pol_last);
-            if constexpr (use_v) {
-                cp_async16(base + L::kVu * kLsmChunk + e, Vu + i, pol_first);
-                if (gram) cp_async16(base + L::kVg * kLsmChunk + e, Vg + i, pol_last);
+            if (rows) {
+                cp_async16(base + L::kSu * kLsmChunk + e, Su + i, pol_first);
+                if (gram) cp_async16(base + L::kSg * kLsmChunk + e, Sg + i, pol_last);
+                if constexpr (use_v) {
+                    cp_async16(base + L::kVu * kLsmChunk + e, Vu + i, pol_first);
+                    if (gram) cp_async16(base + L::kVg * kLsmChunk + e, Vg + i, pol_last);
+                }
             }
+            if (flows && !init) cp_async16(base + L::kCf * kLsmChunk + e, cf + i, pol_last);
         }
     };
 
+    // The first chunk's slab rows do not depend on the previous date: fetch them
+    // before waiting for it; the cash flows and this date's coefficients after.
     int64_t chunk = blockIdx.x;
-    if (chunk < n_chunks) issue(chunk, 0);
+    if (chunk < n_chunks) issue(chunk, 0, true, false);
+    pdl_wait_preceding();
+    double cu[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) cu[i] = init ? 0.0 : coeffs[d_upd * kMaxCoef + i];
+    if (chunk < n_chunks) issue(chunk, 0, false, true);
     cp_async_commit();
     for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {
         const int64_t next = chunk + gridDim.x;
-        if (next < n_chunks) issue(next, (k + 1) & 1);
+        if (next < n_chunks) issue(next, (k + 1) & 1, true, true);
         cp_async_commit();
         cp_async_wait_all_but_one();  // this thread's copies of `chunk` have landed
         __syncthreads();              // ... and every other thread's
@@ -699,9 +718,22 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmAr
     lsm_sweep_kernel<R, BASIS><<<sgrid, kLsmBlock, smem, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre,
                                                               block_sums, done, flags);
     ++*launches;
+    // later dates: programmatic dependent launches (each may start while the
+    // previous date's last block solves; it waits in-kernel before reading)
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(sgrid));
+    cfg.blockDim = dim3(kLsmBlock);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     for (int d = D - 2; d >= 1; --d) {
-        lsm_sweep_kernel<R, BASIS><<<sgrid, kLsmBlock, smem, s>>>(a, S, V, cf, d, 0, d - 1, coeffs, centre,
-                                                                  block_sums, done, flags);
+        e = cudaLaunchKernelEx(&cfg, lsm_sweep_kernel<R, BASIS>, a, S, V, cf, d, 0, d - 1, coeffs, centre, block_sums,
+                               done, flags);
+        if (e != cudaSuccess) return e;
         ++*launches;
     }
     lsm_final_kernel<R, BASIS><<<grid, kLsmBlock, 0, s>>>(a, S, V, cf, 0, coeffs, centre, block_moments);
