@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--skip-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--shape", default=None,
+                    help="launch shape 'tiles_per_warp,guided_tail,paths_per_lane' instead of the autotuner")
     ap.add_argument("--paths", type=int, default=N_PATHS,
                     help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
     ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve"], default="bates5",
@@ -403,7 +405,11 @@ def main() -> None:
 
     # ---- launch shape: the engine's autotuner on the workload itself (untimed)
     tuned = None
-    if not args.no_autotune:
+    if args.shape:
+        tpw, tail, lanes = (int(x) for x in args.shape.split(","))
+        h.tune_set(contract.precision, contract.model, contract.scheme, tpw, bool(tail), lanes)
+        tuned = {"tiles_per_warp": tpw, "guided_tail": tail, "paths_per_lane": lanes, "set_by": "--shape"}
+    elif not args.no_autotune:
         rep = h.autotune([contract], None, reps=1)[0]
         tuned = {"tiles_per_warp": rep["tiles_per_warp"], "guided_tail": rep["guided_tail"],
                  "paths_per_lane": rep["paths_per_lane"],

@@ -156,7 +156,8 @@ static double draw_uniform_d(Draws *d, int as_float) {
         return d->u[d->used++];
     }
     /* Philox layout of the Poisson uniforms of step n (engine's draw layout):
-       1st: domain 2, block n/4, word n%4; 2nd, 3rd: domain 1, block n, words z, w;
+       1st: w_first (FP64 domain 2, block n/4, word n%4; FP32 see run_path_sign);
+       2nd, 3rd: domain 1, block n, words z, w;
        k-th (k >= 4, 1-based): domain 3 + (k-4)/4, block n, word (k-4)%4. */
     const int k = d->used++;
     uint32_t word;
@@ -382,7 +383,15 @@ static void run_path_sign(const qk_contract *c, const Inv *p, const InvF *pf, ui
         const uint32_t wb = (n & 1) ? w[3] : w[1];
         if (c->model == QK_BATES) {
             if ((n & 3) == 0) philox_block((uint32_t)(n >> 2), path, stream, 2u, k0, k1, wp);
-            d.w_first = wp[n & 3];
+            if (fp32) {
+                /* FP32: 23-bit uniform from the low 9 bits of the two normal words and the
+                   top 5 bits of the domain-2 word (the engine fetches that word only when
+                   the first 18 bits cannot decide the jump test) */
+                const uint32_t hi = ((wa & 0x1FFu) << 9) | (wb & 0x1FFu);
+                d.w_first = ((hi << 5) | (wp[n & 3] >> 27)) << 9;
+            } else {
+                d.w_first = wp[n & 3];
+            }
         }
         if (fp32) {
             float z1, z2;

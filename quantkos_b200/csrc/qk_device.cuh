@@ -162,12 +162,17 @@ __device__ __forceinline__ R rmin(R a, R b) { return fmin(a, b); }
 //
 // Philox layout per path p of stream s (counter = (block, p, s, domain)):
 //   normal pair of step n:        domain 0, block floor(n/2), words (x,y) if n even, (z,w) if odd;
-//   1st Poisson uniform of step n: domain 2, block floor(n/4), word n mod 4;
+//   1st Poisson uniform of step n: FP64 domain 2, block floor(n/4), word n mod 4;
+//                                  FP32 23 bits: the low 9 bits of each of the step's two
+//                                  normal words (18 bits), then the top 5 bits of that
+//                                  domain-2 word, drawn only when the first 18 cannot
+//                                  decide the jump test;
 //   jump normal of step n:         domain 1, block n, Box-Muller of words (x,y), first output;
 //   Poisson uniforms 2, 3:         domain 1, block n, words z, w;
 //   Poisson uniform k >= 4:        domain 3 + (k-4)/4, block n, word (k-4) mod 4.
-// A step costs half a Philox block for the normals and, under Bates, a quarter
-// block for the jump test; the rest is drawn only on the rare steps with a jump.
+// A step costs half a Philox block for the normals and, under Bates in FP64, a
+// quarter block for the jump test (in FP32 nearly nothing); the rest is drawn only
+// on the rare steps with a jump.
 // ============================================================================
 template <class R>
 struct PhiloxJumpDraws {

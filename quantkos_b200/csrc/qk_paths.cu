@@ -80,6 +80,40 @@ __device__ __forceinline__ bool jump_test(uint32_t word, const StepConst<R> &p, 
     }
 }
 
+// FP32 first Poisson uniform of step n: 23 bits k = hi:lo.  hi (18 bits) are the low
+// 9 bits of the step's two normal words — FP32 Box-Muller reads only their top 23
+// bits, so hi is independent of the normals — and lo (5 bits) the top bits of word
+// n mod 4 of block (n/4, path, stream, domain 2), drawn only when hi alone cannot
+// decide the jump test (hi >= kmin >> 5: about lambda dt of the steps).  Returns a
+// word whose top 23 bits hold k (what jump_test and u01 read); below the threshold
+// the low part is left zero, which cannot change the (negative) test.
+template <class Gen>
+__device__ __forceinline__ uint32_t poisson_word_f32(uint32_t wa, uint32_t wb, uint32_t kmin, const Gen &gen,
+                                                     uint32_t path, uint32_t stream, int n) {
+    const uint32_t hi = ((wa & 0x1FFu) << 9) | (wb & 0x1FFu);
+    if (hi < (kmin >> 5)) return hi << 14;
+    const U4 q = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
+    const int j = n & 3;
+    const uint32_t w = j == 0 ? q.x : (j == 1 ? q.y : (j == 2 ? q.z : q.w));
+    return ((hi << 5) | (w >> 27)) << 9;
+}
+
+// Words of the first Poisson uniforms of steps n and n+1 (n even) from the normal
+// block w of those steps: FP32 as above; FP64 word n mod 4 of the domain-2 block wp
+// (fetched by the caller every fourth step).
+template <class R, class Gen>
+__device__ __forceinline__ void poisson_words(const U4 &w, const U4 &wp, uint32_t kmin, const Gen &gen,
+                                              uint32_t path, uint32_t stream, int n, uint32_t &p0, uint32_t &p1) {
+    if constexpr (sizeof(R) == 4) {
+        p0 = poisson_word_f32(w.x, w.y, kmin, gen, path, stream, n);
+        p1 = poisson_word_f32(w.z, w.w, kmin, gen, path, stream, n + 1);
+    } else {
+        const bool lo = (n & 3) == 0;
+        p0 = lo ? wp.x : wp.z;
+        p1 = lo ? wp.y : wp.w;
+    }
+}
+
 template <class R, int MODEL, int SCHEME>
 __device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st, uint32_t wa, uint32_t wb,
                                          uint32_t wpois, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path,
@@ -111,23 +145,30 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
         int n = n0;
         for (; n + 1 < n1; n += 2) {
             const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u});
+            uint32_t pw0 = 0u, pw1 = 0u;
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
+                if constexpr (sizeof(R) == 8) {
+                    if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
+                }
+                poisson_words<R>(w, wp, kmin, gen, path, stream, n, pw0, pw1);
             }
-            const bool lo = (n & 3) == 0;
-            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, lo ? wp.x : wp.z, kmin, k0, k1, path, stream, n);
+            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
             track(st, blk);
             sink(n, st.S, st.v);
-            one_step<R, MODEL, SCHEME>(p, st, w.z, w.w, lo ? wp.y : wp.w, kmin, k0, k1, path, stream, n + 1);
+            one_step<R, MODEL, SCHEME>(p, st, w.z, w.w, pw1, kmin, k0, k1, path, stream, n + 1);
             track(st, blk);
             sink(n + 1, st.S, st.v);
         }
         if (n < n1) {
             const U4 w = gen(U4{static_cast<uint32_t>(n >> 1), path, stream, 0u});
+            uint32_t pw0 = 0u, pw1 = 0u;
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
+                if constexpr (sizeof(R) == 8) {
+                    if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
+                }
+                poisson_words<R>(w, wp, kmin, gen, path, stream, n, pw0, pw1);
             }
-            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, (n & 3) == 0 ? wp.x : wp.z, kmin, k0, k1, path, stream, n);
+            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
             track(st, blk);
             sink(n, st.S, st.v);
         }
@@ -197,19 +238,23 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
             const U4 wa = gen(U4{static_cast<uint32_t>(n >> 1), path_a, stream, 0u});
             U4 wb{0u, 0u, 0u, 0u};
             if constexpr (!NEG) wb = gen(U4{static_cast<uint32_t>(n >> 1), path_b, stream, 0u});
+            uint32_t qa0 = 0u, qa1 = 0u, qb0 = 0u, qb1 = 0u;
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) {
-                    pa = gen(U4{static_cast<uint32_t>(n >> 2), path_a, stream, 2u});
-                    if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
+                if constexpr (sizeof(R) == 8) {
+                    if ((n & 3) == 0) {
+                        pa = gen(U4{static_cast<uint32_t>(n >> 2), path_a, stream, 2u});
+                        if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
+                    }
                 }
+                poisson_words<R>(wa, pa, kmin, gen, path_a, stream, n, qa0, qa1);
+                if constexpr (!NEG) poisson_words<R>(wb, pb, kmin, gen, path_b, stream, n, qb0, qb1);
             }
-            const bool lo = (n & 3) == 0;
-            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, lo ? pa.x : pa.z, lo ? pb.x : pb.z,
-                                                kmin, k0, k1, path_a, path_b, stream, n);
+            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
+                                                path_b, stream, n);
             track(a, blk_a);
             track(b, blk_b);
-            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.z, wa.w, wb.z, wb.w, lo ? pa.y : pa.w, lo ? pb.y : pb.w,
-                                                kmin, k0, k1, path_a, path_b, stream, n + 1);
+            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.z, wa.w, wb.z, wb.w, qa1, qb1, kmin, k0, k1, path_a,
+                                                path_b, stream, n + 1);
             track(a, blk_a);
             track(b, blk_b);
         }
@@ -217,15 +262,19 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
             const U4 wa = gen(U4{static_cast<uint32_t>(n >> 1), path_a, stream, 0u});
             U4 wb{0u, 0u, 0u, 0u};
             if constexpr (!NEG) wb = gen(U4{static_cast<uint32_t>(n >> 1), path_b, stream, 0u});
+            uint32_t qa0 = 0u, qa1 = 0u, qb0 = 0u, qb1 = 0u;
             if constexpr (MODEL == kBates) {
-                if ((n & 3) == 0) {
-                    pa = gen(U4{static_cast<uint32_t>(n >> 2), path_a, stream, 2u});
-                    if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
+                if constexpr (sizeof(R) == 8) {
+                    if ((n & 3) == 0) {
+                        pa = gen(U4{static_cast<uint32_t>(n >> 2), path_a, stream, 2u});
+                        if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
+                    }
                 }
+                poisson_words<R>(wa, pa, kmin, gen, path_a, stream, n, qa0, qa1);
+                if constexpr (!NEG) poisson_words<R>(wb, pb, kmin, gen, path_b, stream, n, qb0, qb1);
             }
-            const bool lo = (n & 3) == 0;
-            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, lo ? pa.x : pa.z, lo ? pb.x : pb.z,
-                                                kmin, k0, k1, path_a, path_b, stream, n);
+            one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
+                                                path_b, stream, n);
             track(a, blk_a);
             track(b, blk_b);
         }
