@@ -313,6 +313,135 @@ __device__ __forceinline__ void step_qe(const StepConst<R> &p, R &S, R &v, R Zv,
     v = vn;
 }
 
+// ----------------------------------------------------------------------------
+// FP32 QE and Euler with an explicit rounding order.  Every FP32 operation below
+// is an IEEE-rounded intrinsic (no compiler contraction), and the paired two-path
+// forms further down perform the same operations on float2 pairs with the sm_100
+// paired FP32 instructions, so one path gives the same bits whichever form
+// simulates it.  Same algebra as the generic steps above.
+__device__ __forceinline__ void qe_quadratic_f32(const StepConst<float> &p, float m, float m2, float s2, float Zv,
+                                                 float &vn, float &logM) {
+    const float two_ip = __fmul_rn(__fmul_rn(2.0f, m2), ptx_rcp(s2));
+    const float t1 = __fadd_rn(two_ip, -1.0f);
+    const float b2 = __fadd_rn(t1, ptx_sqrt(__fmul_rn(two_ip, t1)));
+    const float a = __fmul_rn(m, ptx_rcp(__fadd_rn(1.0f, b2)));
+    const float bz = __fadd_rn(ptx_sqrt(b2), Zv);
+    vn = __fmul_rn(__fmul_rn(a, bz), bz);
+    const float Aa = fminf(__fmul_rn(p.A, a), __fmaf_rn(-p.eps, a, 0.5f));
+    const float term = __fmaf_rn(-2.0f, Aa, 1.0f);
+    logM = __fmaf_rn(__fmul_rn(Aa, b2), ptx_rcp(term), __fmul_rn(-0.5f * Math<float>::kLn2, ptx_lg2(term)));
+}
+
+__device__ __forceinline__ void qe_spot_f32(const StepConst<float> &p, float &S, float v, float vn, float logM,
+                                            float Zind) {
+    const float K0n = __fmaf_rn(p.K1_half_K3, v, logM);  // -K0
+    const float isig = __fmaf_rn(p.K3, v, __fmul_rn(p.K4, vn));
+    const float e12 = __fadd_rn(__fadd_rn(p.r_minus_q_dt, -K0n), __fmaf_rn(p.K1, v, __fmul_rn(p.K2, vn)));
+    const float ex = __fmaf_rn(ptx_sqrt(isig), Zind, e12);
+    S = __fmul_rn(S, ptx_ex2(__fmul_rn(ex, Math<float>::kLog2e)));
+}
+
+template <>
+__device__ __forceinline__ void step_qe<float>(const StepConst<float> &p, float &S, float &v, float Zv, float Zind) {
+    const float m = __fmaf_rn(v, p.exp_mkdt, p.theta_m);
+    const float s2 = __fmaf_rn(v, p.s2f1, p.s2f2);
+    float vn, logM;
+    if (m <= p.eps) {
+        vn = 0.0f;
+        logM = 0.0f;
+    } else {
+        const float m2 = __fmul_rn(m, m);
+        if (s2 <= __fmul_rn(p.eps, m2)) {
+            vn = m;
+            logM = 0.0f;
+        } else if (s2 <= __fmul_rn(p.psi_c, m2)) {
+            qe_quadratic_f32(p, m, m2, s2, Zv, vn, logM);
+        } else {
+            // exponential branch (rare at the usual parameters): as the generic step
+            const float inv_m = ptx_rcp(m);
+            const float psi = s2 * inv_m * inv_m;
+            const float pz = Math<float>::div(psi - 1.0f, psi + 1.0f);
+            const float beta = (1.0f - pz) * inv_m;
+            const float U = 0.5f * (1.0f + erff(Zv * p.inv_sqrt2));
+            if (U <= pz) {
+                vn = 0.0f;
+            } else {
+                const float safe_U = fminf(U, 1.0f - p.eps);
+                vn = Math<float>::div(Math<float>::log(Math<float>::div(1.0f - pz, 1.0f - safe_U)), beta);
+            }
+            const float safe_A = fminf(p.A, beta - p.eps);
+            const float M = pz + Math<float>::div(beta * (1.0f - pz), beta - safe_A);
+            logM = Math<float>::log(M);
+        }
+    }
+    qe_spot_f32(p, S, v, vn, logM, Zind);
+    v = vn;
+}
+
+template <>
+__device__ __forceinline__ void step_euler<float>(const StepConst<float> &p, float &S, float &v, float Z1, float Z2) {
+    const float ZS = __fmaf_rn(p.rho, Z1, __fmul_rn(p.rho_c, Z2));
+    const float sqv = ptx_sqrt(v);
+    const float ex = __fmaf_rn(__fmul_rn(sqv, p.sqrt_dt), ZS, __fmaf_rn(v, -p.half_dt, p.r_minus_q_dt));
+    S = __fmul_rn(S, ptx_ex2(__fmul_rn(ex, Math<float>::kLog2e)));
+    v = fmaxf(__fmaf_rn(__fmul_rn(p.sigma_sqrt_dt, sqv), Z1, __fmaf_rn(v, p.one_minus_k_dt, p.k_theta_dt)), 0.0f);
+}
+
+// Paired FP32: component-wise IEEE operations on two paths at once.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 rcp2(float2 x) { return make_float2(ptx_rcp(x.x), ptx_rcp(x.y)); }
+__device__ __forceinline__ float2 sqrt2(float2 x) { return make_float2(ptx_sqrt(x.x), ptx_sqrt(x.y)); }
+__device__ __forceinline__ float2 lg2_2(float2 x) { return make_float2(ptx_lg2(x.x), ptx_lg2(x.y)); }
+__device__ __forceinline__ float2 ex2_2(float2 x) { return make_float2(ptx_ex2(x.x), ptx_ex2(x.y)); }
+__device__ __forceinline__ float2 min2(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+__device__ __forceinline__ float2 max0_2(float2 a) { return make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)); }
+
+// QE step of two paths (spot S, variance v as pairs): paired when both take the
+// quadratic branch (the common case), otherwise each path through step_qe<float>.
+__device__ __forceinline__ void step_qe_two_f32(const StepConst<float> &p, float2 &S, float2 &v, float2 Zv,
+                                                float2 Zind) {
+    const float2 m = __ffma2_rn(v, f2(p.exp_mkdt), f2(p.theta_m));
+    const float2 s2 = __ffma2_rn(v, f2(p.s2f1), f2(p.s2f2));
+    const float2 m2 = __fmul2_rn(m, m);
+    const float2 em2 = __fmul2_rn(f2(p.eps), m2);
+    const float2 pm2 = __fmul2_rn(f2(p.psi_c), m2);
+    const bool quad = m.x > p.eps && m.y > p.eps && s2.x > em2.x && s2.y > em2.y && s2.x <= pm2.x && s2.y <= pm2.y;
+    if (!quad) {
+        step_qe<float>(p, S.x, v.x, Zv.x, Zind.x);
+        step_qe<float>(p, S.y, v.y, Zv.y, Zind.y);
+        return;
+    }
+    // qe_quadratic_f32, paired
+    const float2 two_ip = __fmul2_rn(__fmul2_rn(f2(2.0f), m2), rcp2(s2));
+    const float2 t1 = __fadd2_rn(two_ip, f2(-1.0f));
+    const float2 b2 = __fadd2_rn(t1, sqrt2(__fmul2_rn(two_ip, t1)));
+    const float2 a = __fmul2_rn(m, rcp2(__fadd2_rn(f2(1.0f), b2)));
+    const float2 bz = __fadd2_rn(sqrt2(b2), Zv);
+    const float2 vn = __fmul2_rn(__fmul2_rn(a, bz), bz);
+    const float2 Aa = min2(__fmul2_rn(f2(p.A), a), __ffma2_rn(f2(-p.eps), a, f2(0.5f)));
+    const float2 term = __ffma2_rn(f2(-2.0f), Aa, f2(1.0f));
+    const float2 logM = __ffma2_rn(__fmul2_rn(Aa, b2), rcp2(term),
+                                   __fmul2_rn(f2(-0.5f * Math<float>::kLn2), lg2_2(term)));
+    // qe_spot_f32, paired
+    const float2 K0n = __ffma2_rn(f2(p.K1_half_K3), v, logM);
+    const float2 isig = __ffma2_rn(f2(p.K3), v, __fmul2_rn(f2(p.K4), vn));
+    const float2 e12 = __fadd2_rn(__fadd2_rn(f2(p.r_minus_q_dt), __fmul2_rn(K0n, f2(-1.0f))),
+                                  __ffma2_rn(f2(p.K1), v, __fmul2_rn(f2(p.K2), vn)));
+    const float2 ex = __ffma2_rn(sqrt2(isig), Zind, e12);
+    S = __fmul2_rn(S, ex2_2(__fmul2_rn(ex, f2(Math<float>::kLog2e))));
+    v = vn;
+}
+
+__device__ __forceinline__ void step_euler_two_f32(const StepConst<float> &p, float2 &S, float2 &v, float2 Z1,
+                                                   float2 Z2) {
+    const float2 ZS = __ffma2_rn(f2(p.rho), Z1, __fmul2_rn(f2(p.rho_c), Z2));
+    const float2 sqv = sqrt2(v);
+    const float2 ex = __ffma2_rn(__fmul2_rn(sqv, f2(p.sqrt_dt)), ZS, __ffma2_rn(v, f2(-p.half_dt), f2(p.r_minus_q_dt)));
+    S = __fmul2_rn(S, ex2_2(__fmul2_rn(ex, f2(Math<float>::kLog2e))));
+    v = max0_2(__ffma2_rn(__fmul2_rn(f2(p.sigma_sqrt_dt), sqv), Z1,
+                          __ffma2_rn(v, f2(p.one_minus_k_dt), f2(p.k_theta_dt))));
+}
+
 template <class R, int SCHEME>
 __device__ __forceinline__ void heston_step(const StepConst<R> &p, R &S, R &v, R Z1, R Z2) {
     if constexpr (SCHEME == kEuler) {

@@ -31,8 +31,10 @@ constexpr int kMergeChunkTiles = 512;
 // level 2 reduces each task's chunk records into out[task][QK_MAX_PAYOFFS].
 cudaError_t launch_merge_two_level(int n_tasks, int64_t n_chunks, cudaStream_t s, const TaskDev *tasks,
                                    const Moments *partials, Moments *chunks, TaskMoments *out);
+// paths_per_thread 2: each thread simulates two consecutive paths (same values).
 cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t seed, cudaStream_t s, const TaskDev *task,
-                              int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld);
+                              int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld,
+                              int paths_per_thread = 1);
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
                               int umax, int n, double *S_out, double *v_out, int *status);
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);

@@ -852,9 +852,10 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         const bool use_v = b.lsm_basis == QK_LSM_POLY_SV;
         // forward: exercise-date slabs
         QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k], h->stream));
+        // FP32: two paths per thread, stepped as pairs
         QK_CUDA_LSM(launch_slab_paths(prec, b.model, b.scheme, b.seed, h->stream,
                                       static_cast<const TaskDev *>(L.task.ptr) + k, 0, b.n_paths, stride, L.slab_S.ptr,
-                                      use_v ? L.slab_v.ptr : nullptr, ld));
+                                      use_v ? L.slab_v.ptr : nullptr, ld, prec == QK_FP32 ? 2 : 1));
         h->lsm_launches++;
         QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 1], h->stream));
         LsmArgs a;

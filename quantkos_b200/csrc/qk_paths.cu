@@ -46,6 +46,35 @@ struct SlabSink {
     }
 };
 
+// Two paths per thread: stores S (and v) of paths a and b (b only if it exists).
+struct NoSink2 {
+    template <class R>
+    __device__ __forceinline__ void operator()(int, R, R, R, R) const {}
+};
+
+template <class R>
+struct SlabSink2 {
+    R *slab_S;
+    R *slab_v;
+    int64_t ld;
+    int64_t pos;   // slab index of path a's next stored date; path b is the next column
+    int stride;
+    int left;
+    bool has_b;
+    __device__ __forceinline__ void operator()(int, R Sa, R va, R Sb, R vb) {
+        if (--left == 0) {
+            left = stride;
+            slab_S[pos] = Sa;
+            if (has_b) slab_S[pos + 1] = Sb;
+            if (slab_v) {
+                slab_v[pos] = va;
+                if (has_b) slab_v[pos + 1] = vb;
+            }
+            pos += ld;
+        }
+    }
+};
+
 // Steps are taken in chunks of kSumChunk; the Asian running sum is accumulated in
 // the working precision inside a chunk and folded into the FP64 sum after it.
 constexpr int kSumChunk = 16;
@@ -185,14 +214,25 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
                                              uint32_t wa2, uint32_t wb1, uint32_t wb2, uint32_t pois_a,
                                              uint32_t pois_b, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path_a,
                                              uint32_t path_b, uint32_t stream, int n) {
-    R za1, za2;
+    R za1, za2, zb1, zb2;
     Math<R>::box_muller(wa1, wa2, za1, za2);
-    heston_step<R, SCHEME>(p, a.S, a.v, za1, za2);
     if constexpr (NEG) {
-        heston_step<R, SCHEME>(p, b.S, b.v, -za1, -za2);
+        zb1 = -za1;
+        zb2 = -za2;
     } else {
-        R zb1, zb2;
         Math<R>::box_muller(wb1, wb2, zb1, zb2);
+    }
+    if constexpr (sizeof(R) == 4 && SCHEME != kMilstein) {
+        // both paths in one paired FP32 step
+        float2 S2 = make_float2(a.S, b.S), v2 = make_float2(a.v, b.v);
+        if constexpr (SCHEME == kQE) step_qe_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
+        else step_euler_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
+        a.S = S2.x;
+        b.S = S2.y;
+        a.v = v2.x;
+        b.v = v2.y;
+    } else {
+        heston_step<R, SCHEME>(p, a.S, a.v, za1, za2);
         heston_step<R, SCHEME>(p, b.S, b.v, zb1, zb2);
     }
     if constexpr (MODEL == kBates) {
@@ -220,10 +260,11 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
     }
 }
 
-template <class R, int MODEL, int SCHEME, bool NEG, class Gen>
+template <class R, int MODEL, int SCHEME, bool NEG, class Gen, class Sink2>
 __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
                                              uint32_t k0, uint32_t k1, uint32_t path_a, uint32_t path_b,
-                                             uint32_t stream, uint32_t kmin, PathState<R> &a, PathState<R> &b) {
+                                             uint32_t stream, uint32_t kmin, PathState<R> &a, PathState<R> &b,
+                                             Sink2 &&sink) {
     a.S = b.S = S0;
     a.v = b.v = v0;
     a.ssum = b.ssum = 0.0;
@@ -253,10 +294,12 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
                                                 path_b, stream, n);
             track(a, blk_a);
             track(b, blk_b);
+            sink(n, a.S, a.v, b.S, b.v);
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.z, wa.w, wb.z, wb.w, qa1, qb1, kmin, k0, k1, path_a,
                                                 path_b, stream, n + 1);
             track(a, blk_a);
             track(b, blk_b);
+            sink(n + 1, a.S, a.v, b.S, b.v);
         }
         if (n < n1) {
             const U4 wa = gen(U4{static_cast<uint32_t>(n >> 1), path_a, stream, 0u});
@@ -277,6 +320,7 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
                                                 path_b, stream, n);
             track(a, blk_a);
             track(b, blk_b);
+            sink(n, a.S, a.v, b.S, b.v);
         }
         a.ssum += static_cast<double>(blk_a);
         b.ssum += static_cast<double>(blk_b);
@@ -383,10 +427,10 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
                 if (active) {
                     if constexpr (UK) {
                         simulate_two<R, MODEL, SCHEME, NEG>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1, pa, pb, stream,
-                                                            kmin, sa, sb);
+                                                            kmin, sa, sb, NoSink2{});
                     } else {
                         simulate_two<R, MODEL, SCHEME, NEG>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1, pa, pb,
-                                                            stream, kmin, sa, sb);
+                                                            stream, kmin, sa, sb, NoSink2{});
                     }
                 } else {
                     sa.S = sa.smax = sa.smin = sb.S = sb.smax = sb.smin = R(0);
@@ -594,8 +638,38 @@ __global__ void __launch_bounds__(kPathBlock) slab_paths_kernel(const TaskDev *_
                                     t.key1, static_cast<uint32_t>(first_path + i), t.stream, t.jump_kmin, st, sink);
 }
 
+// Two paths per thread (first + 2i and first + 2i + 1), interleaved and, in FP32,
+// stepped as pairs; same values as the one-path kernel.
+template <class R, int MODEL, int SCHEME>
+__global__ void __launch_bounds__(kPathBlock) slab_paths_two_kernel(const TaskDev *__restrict__ task,
+                                                                   int64_t first_path, int64_t count, int stride,
+                                                                   R *__restrict__ slab_S, R *__restrict__ slab_v,
+                                                                   int64_t ld, const PhiloxRoundKeys rk) {
+    const int64_t i = 2 * (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x);
+    if (i >= count) return;
+    const TaskDev &t = *task;
+    const StepConst<R> p = task_const<R>(t);
+    SlabSink2<R> sink{slab_S, slab_v, ld, i, stride, stride, i + 1 < count};
+    PathState<R> sa, sb;
+    const uint32_t pa = static_cast<uint32_t>(first_path + i);
+    simulate_two<R, MODEL, SCHEME, false>(p, static_cast<R>(t.S0), static_cast<R>(t.v0), t.n_steps, ParamKeys{rk},
+                                          t.key0, t.key1, pa, pa + 1u, t.stream, t.jump_kmin, sa, sb, sink);
+}
+
 template <class R>
 using SlabKernel = void (*)(const TaskDev *, int64_t, int64_t, int, R *, R *, int64_t, const PhiloxRoundKeys);
+
+template <class R>
+SlabKernel<R> slab_two_kernel_for(int model, int scheme) {
+    switch (model * 3 + scheme) {
+        case 0: return slab_paths_two_kernel<R, kHeston, kEuler>;
+        case 1: return slab_paths_two_kernel<R, kHeston, kMilstein>;
+        case 2: return slab_paths_two_kernel<R, kHeston, kQE>;
+        case 3: return slab_paths_two_kernel<R, kBates, kEuler>;
+        case 4: return slab_paths_two_kernel<R, kBates, kMilstein>;
+        default: return slab_paths_two_kernel<R, kBates, kQE>;
+    }
+}
 
 template <class R>
 SlabKernel<R> slab_kernel_for(int model, int scheme) {
@@ -689,10 +763,22 @@ cudaError_t launch_merge_two_level(int n_tasks, int64_t n_chunks, cudaStream_t s
 }
 
 cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t seed, cudaStream_t s, const TaskDev *task,
-                              int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld) {
-    const int64_t blocks = (count + kPathBlock - 1) / kPathBlock;
+                              int64_t first_path, int64_t count, int stride, void *slab_S, void *slab_v, int64_t ld,
+                              int paths_per_thread) {
     const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
                                                  static_cast<uint32_t>(seed >> 32));
+    if (paths_per_thread == 2) {
+        const int64_t threads = (count + 1) / 2;
+        const unsigned blocks2 = static_cast<unsigned>((threads + kPathBlock - 1) / kPathBlock);
+        if (precision == QK_FP32)
+            slab_two_kernel_for<float>(model, scheme)<<<blocks2, kPathBlock, 0, s>>>(
+                task, first_path, count, stride, static_cast<float *>(slab_S), static_cast<float *>(slab_v), ld, rk);
+        else
+            slab_two_kernel_for<double>(model, scheme)<<<blocks2, kPathBlock, 0, s>>>(
+                task, first_path, count, stride, static_cast<double *>(slab_S), static_cast<double *>(slab_v), ld, rk);
+        return cudaGetLastError();
+    }
+    const int64_t blocks = (count + kPathBlock - 1) / kPathBlock;
     if (precision == QK_FP32)
         slab_kernel_for<float>(model, scheme)<<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(
             task, first_path, count, stride, static_cast<float *>(slab_S), static_cast<float *>(slab_v), ld, rk);
