@@ -286,6 +286,8 @@ typedef struct qk_config {
     char out_dir[256], paths_file[256], log_file[256];
     int32_t precision, engine, lsm_basis, lsm_dates, vega_mode; /* engine extensions */
     uint64_t stream;
+    int32_t antithetic;                                         /* MC.Antithetic (extension) */
+    int32_t reserved_;
 } qk_config;
 
 /* Defaults of UInputs (Config.hpp:50-623) plus engine extensions (FP64, plain). */

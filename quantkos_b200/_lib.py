@@ -113,7 +113,7 @@ class Config(C.Structure):
         ("verbosity", C.c_int32), ("format", C.c_int32),
         ("out_dir", C.c_char * 256), ("paths_file", C.c_char * 256), ("log_file", C.c_char * 256),
         ("precision", C.c_int32), ("engine", C.c_int32), ("lsm_basis", C.c_int32), ("lsm_dates", C.c_int32),
-        ("vega_mode", C.c_int32), ("stream", C.c_uint64),
+        ("vega_mode", C.c_int32), ("stream", C.c_uint64), ("antithetic", C.c_int32), ("reserved_", C.c_int32),
     ]
 
 

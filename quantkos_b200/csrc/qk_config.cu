@@ -271,6 +271,7 @@ qk_status fill_config(const YamlDoc &d, qk_config *c) {
     QK_TRY(get_int(d, "MC.LSM_Dates", &c->lsm_dates));
     QK_TRY(get_int(d, "MC.Vega_Mode", &c->vega_mode));
     QK_TRY(get_int(d, "MC.Stream", &c->stream));
+    QK_TRY(get_bool(d, "MC.Antithetic", &c->antithetic));
     // 9. Output (optional)
     QK_TRY(get_enum(d, "Output.Verbosity", kVerbosity, &c->verbosity));
     if (has(d, "Output.out_dir")) copy_str(c->out_dir, d.values.at("Output.out_dir"));
@@ -365,6 +366,7 @@ qk_status qk_config_default(qk_config *c) {
     c->lsm_dates = 0;
     c->vega_mode = 0;
     c->stream = 0;
+    c->antithetic = 0;
     return QK_OK;
 }
 
@@ -440,6 +442,7 @@ qk_status qk_config_to_contract(const qk_config *c, qk_contract *k, qk_greeks *g
     k->n_paths = c->n_paths;
     k->seed = c->seed;
     k->stream = c->stream;
+    k->antithetic = c->antithetic;
     k->precision = c->precision;
     k->n_payoffs = 1;
     k->payoffs[0].type = c->opt_type;

@@ -177,3 +177,16 @@ def test_validate_greek_bumps(qk):
     assert lib.qk_validate(C.byref(k), C.byref(g)) == qk.lib.QK_OK
     k.n_paths = 0
     assert lib.qk_validate(C.byref(k), None) == qk.lib.QK_ERR_INVALID_ARG
+
+
+def test_parser_engine_extension_keys(qk):
+    """Extension keys (absent from the reference's configs; defaults keep its behaviour)."""
+    u = qk.Parser.parse_string(CONFIG_YAML)
+    assert u.precision == qk.FP64 and u.engine == 0 and u.antithetic == 0 and u.stream == 0
+    y = CONFIG_YAML.replace("  RNG_Seed: 88471920573105",
+                            "  RNG_Seed: 88471920573105\n  Precision: FP32\n  Engine: batch\n  Antithetic: true\n"
+                            "  Stream: 7\n  Vega_Mode: 1")
+    u = qk.Parser.parse_string(y)
+    assert u.precision == qk.FP32 and u.engine == 1 and u.antithetic == 1 and u.stream == 7 and u.vega_mode == 1
+    k, g = u.to_contract()
+    assert k.antithetic == 1 and k.precision == qk.FP32 and k.stream == 7 and g.vega_mode == 1

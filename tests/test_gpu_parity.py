@@ -340,3 +340,25 @@ def test_antithetic_reduces_error_and_validates(qk, handle, oracle):
     with pytest.raises(RuntimeError, match="antithetic"):
         qk.price_batch([qk.make_contract(antithetic=True, **{**base, "payoffs": [qk.payoff(qk.AMERICAN, qk.PUT, 100.0)]})],
                        None, handle)
+
+
+@pytest.mark.parametrize("model,scheme", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)])
+def test_lane_modes_simulate_the_same_paths(qk, handle, model, scheme):
+    """A lane carrying two paths (FP32 Euler and QE stepped as pairs on the paired FP32 pipe)
+    and a lane carrying one path simulate bit-identical paths: prices agree to the rounding of
+    the FP64 moment merge, whose grouping of paths differs between the two shapes."""
+    legs = [qk.payoff(qk.EUROPEAN, qk.CALL, 100.0), qk.payoff(qk.ASIAN, qk.CALL, 100.0),
+            qk.payoff(qk.BARRIER_UP_OUT, qk.CALL, 100.0, 130.0), qk.payoff(qk.BINARY_CASH, qk.CALL, 105.0)]
+    c = qk.make_contract(model=model, scheme=scheme, lambda_j=0.3 if model else 0.0, mu_j=-0.05, sigma_j=0.1,
+                         sigma=0.5, n_paths=65_537, n_steps=101, seed=5, precision=qk.FP32, payoffs=legs)
+    out = []
+    try:
+        for lanes in (1, 2):
+            handle.tune_set(qk.FP32, model, scheme, 24, False, lanes)
+            out.append(qk.price_batch([c], None, handle)[0]["legs"])
+    finally:
+        handle.tune_set(qk.FP32, model, scheme, 24, False, 1)
+    for a, b in zip(out[0], out[1]):
+        assert a["price"] == pytest.approx(b["price"], rel=1e-12, abs=1e-15)
+        assert a["std_error"] == pytest.approx(b["std_error"], rel=1e-9)
+        assert a["prob_itm"] == pytest.approx(b["prob_itm"], rel=1e-12, abs=1e-15)
