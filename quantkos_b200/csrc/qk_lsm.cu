@@ -599,10 +599,18 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     __threadfence();
     __shared__ double s_part[kLsmBlock / 32][NACC];
     if (lane < NACC) {
-        double t = 0.0;
-        for (int b = warp; b < static_cast<int>(gridDim.x); b += kLsmBlock / 32)
-            t += __ldcg(block_sums + static_cast<int64_t>(b) * NACC + lane);
-        s_part[warp][lane] = t;
+        // warp w sums blocks w, w + 8, ...: eight independent loads in flight per
+        // iteration (eight partial sums, folded in a fixed order)
+        constexpr int kW = kLsmBlock / 32;
+        const int G = static_cast<int>(gridDim.x);
+        double part[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int b = warp;
+        for (; b + 7 * kW < G; b += 8 * kW) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) part[u] += __ldcg(block_sums + static_cast<int64_t>(b + u * kW) * NACC + lane);
+        }
+        for (; b < G; b += kW) part[0] += __ldcg(block_sums + static_cast<int64_t>(b) * NACC + lane);
+        s_part[warp][lane] = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
     }
     __syncthreads();
     if (threadIdx.x == 0) {
