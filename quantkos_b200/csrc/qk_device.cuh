@@ -387,6 +387,23 @@ __device__ __forceinline__ void step_euler<float>(const StepConst<float> &p, flo
     v = fmaxf(__fmaf_rn(__fmul_rn(p.sigma_sqrt_dt, sqv), Z1, __fmaf_rn(v, p.one_minus_k_dt, p.k_theta_dt)), 0.0f);
 }
 
+// Implicit Milstein variance update with an explicit rounding order.
+__device__ __forceinline__ float milstein_variance_f32(const StepConst<float> &p, float v, float sqv, float Z1) {
+    const float corr = __fmul_rn(p.quarter_sigma_sq_dt, __fmaf_rn(Z1, Z1, -1.0f));
+    const float t = __fadd_rn(__fmaf_rn(__fmul_rn(p.sigma_sqrt_dt, sqv), Z1, __fadd_rn(v, p.k_theta_dt)), corr);
+    return fmaxf(__fmul_rn(p.implicit_den, t), 0.0f);
+}
+
+template <>
+__device__ __forceinline__ void step_milstein<float>(const StepConst<float> &p, float &S, float &v, float Z1,
+                                                     float Z2) {
+    const float ZS = __fmaf_rn(p.rho, Z1, __fmul_rn(p.rho_c, Z2));
+    const float sqv = ptx_sqrt(v);
+    const float ex = __fmaf_rn(__fmul_rn(sqv, p.sqrt_dt), ZS, __fmaf_rn(v, -p.half_dt, p.r_minus_q_dt));
+    S = __fmul_rn(S, ptx_ex2(__fmul_rn(ex, Math<float>::kLog2e)));
+    v = milstein_variance_f32(p, v, sqv, Z1);
+}
+
 // Paired FP32: component-wise IEEE operations on two paths at once.
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 rcp2(float2 x) { return make_float2(ptx_rcp(x.x), ptx_rcp(x.y)); }
@@ -430,6 +447,17 @@ __device__ __forceinline__ void step_qe_two_f32(const StepConst<float> &p, float
     const float2 ex = __ffma2_rn(sqrt2(isig), Zind, e12);
     S = __fmul2_rn(S, ex2_2(__fmul2_rn(ex, f2(Math<float>::kLog2e))));
     v = vn;
+}
+
+// Milstein for two paths: the spot update (the same as Euler's) paired, the
+// variance update per path.
+__device__ __forceinline__ void step_milstein_two_f32(const StepConst<float> &p, float2 &S, float2 &v, float2 Z1,
+                                                      float2 Z2) {
+    const float2 ZS = __ffma2_rn(f2(p.rho), Z1, __fmul2_rn(f2(p.rho_c), Z2));
+    const float2 sqv = sqrt2(v);
+    const float2 ex = __ffma2_rn(__fmul2_rn(sqv, f2(p.sqrt_dt)), ZS, __ffma2_rn(v, f2(-p.half_dt), f2(p.r_minus_q_dt)));
+    S = __fmul2_rn(S, ex2_2(__fmul2_rn(ex, f2(Math<float>::kLog2e))));
+    v = make_float2(milstein_variance_f32(p, v.x, sqv.x, Z1.x), milstein_variance_f32(p, v.y, sqv.y, Z1.y));
 }
 
 __device__ __forceinline__ void step_euler_two_f32(const StepConst<float> &p, float2 &S, float2 &v, float2 Z1,

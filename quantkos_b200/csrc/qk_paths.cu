@@ -222,10 +222,12 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
     } else {
         Math<R>::box_muller(wb1, wb2, zb1, zb2);
     }
-    if constexpr (sizeof(R) == 4 && SCHEME != kMilstein) {
+    if constexpr (sizeof(R) == 4) {
         // both paths in one paired FP32 step
         float2 S2 = make_float2(a.S, b.S), v2 = make_float2(a.v, b.v);
         if constexpr (SCHEME == kQE) step_qe_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
+        else if constexpr (SCHEME == kMilstein)
+            step_milstein_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
         else step_euler_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
         a.S = S2.x;
         b.S = S2.y;

@@ -362,3 +362,26 @@ def test_lane_modes_simulate_the_same_paths(qk, handle, model, scheme):
         assert a["price"] == pytest.approx(b["price"], rel=1e-12, abs=1e-15)
         assert a["std_error"] == pytest.approx(b["std_error"], rel=1e-9)
         assert a["prob_itm"] == pytest.approx(b["prob_itm"], rel=1e-12, abs=1e-15)
+
+
+def test_edge_sizes_match_oracle(qk, handle, oracle):
+    """Ragged and minimal sizes: a single path, partial warps, a single step, an empty request
+    list, and the largest path count a contract may have (32-bit Philox path counter)."""
+    legs = [qk.payoff(qk.EUROPEAN, qk.CALL, 100.0), qk.payoff(qk.ASIAN, qk.PUT, 100.0),
+            qk.payoff(qk.LOOKBACK_FLOATING, qk.CALL, 100.0)]
+    for n_paths, n_steps in ((1, 1), (1, 7), (31, 3), (33, 5), (1000, 1)):
+        for model, scheme in ((0, 2), (1, 0)):
+            k = qk.make_contract(model=model, scheme=scheme, lambda_j=0.5 if model else 0.0, mu_j=-0.1, sigma_j=0.15,
+                                 n_paths=n_paths, n_steps=n_steps, seed=99, precision=qk.FP64, payoffs=legs)
+            want = oracle.price(k)["legs"]
+            for got in (qk.price_plain(k, None, handle)["legs"], qk.price_batch([k], None, handle)[0]["legs"]):
+                for a, b in zip(got, want):
+                    assert a["price"] == pytest.approx(b["price"], rel=1e-9, abs=1e-12), (n_paths, n_steps, a, b)
+                    assert a["prob_itm"] == pytest.approx(b["prob_itm"], rel=1e-12, abs=1e-15)
+                    if n_paths > 1:
+                        assert a["std_error"] == pytest.approx(b["std_error"], rel=1e-6, abs=1e-12)
+                    else:
+                        assert a["std_error"] == 0.0
+    assert qk.price_batch([], None, handle) == []
+    with pytest.raises(ValueError, match="N_Paths"):
+        qk.price_batch([qk.make_contract(n_paths=2 ** 32)], None, handle)
