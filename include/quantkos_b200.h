@@ -140,7 +140,7 @@ typedef struct qk_result {
 /* Device timings of the most recent pricing call on a handle (CUDA events on the handle's stream). */
 typedef struct qk_timing {
     double device_ms;     /* first kernel start to last kernel end */
-    double paths_ms;      /* path-generation kernels */
+    double paths_ms;      /* path-generation kernels (LSM forward kernels of concurrent jobs summed, capped at the call) */
     double reduce_ms;     /* merge / LSM regression kernels */
     int64_t launches;     /* kernels launched by the call */
     double path_steps;    /* path-steps simulated */

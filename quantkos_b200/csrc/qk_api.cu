@@ -647,6 +647,9 @@ qk_status finish_timing(qk_handle *h, double path_steps) {
     QK_CUDA_TRY(cudaEventElapsedTime(&ms_rest, h->ev_paths1, h->ev_end));
     double lsm_paths = 0.0, lsm_sweep = 0.0;
     if (h->lsm_jobs > 0) lsm_timing(h, &lsm_paths, &lsm_sweep);
+    // LSM jobs of one call may overlap on several streams: their summed forward time
+    // is capped at the part of the call outside the forward path kernels
+    lsm_paths = std::min(lsm_paths, std::max(0.0, static_cast<double>(ms_all) - ms_paths));
     h->timing.device_ms = ms_all;
     h->timing.paths_ms = ms_paths + lsm_paths;
     h->timing.reduce_ms = ms_all - ms_paths - lsm_paths;

@@ -55,8 +55,12 @@ struct Plan {
 
 // LSM working set of one task on the device.
 struct LsmArena {
-    DevArena slab_S, slab_v, cashflow, block_sums, coeffs, task, status;
+    DevArena slab_S, slab_v, cashflow, block_sums, coeffs, status;
 };
+
+// American jobs of one call run on up to kLsmLanes streams at once, each stream with
+// its own working set, so that the fixed per-date cost of small jobs overlaps.
+constexpr int kLsmLanes = 4;
 
 }  // namespace qk
 
@@ -68,7 +72,10 @@ struct qk_handle {
     qk::DevArena d_tasks, d_prefix, d_partials, d_moments, d_cursor, d_trace, d_chunks;
     qk::HostArena h_tasks, h_moments, h_lsm;
     qk::DevArena d_lsm_moments;
-    qk::LsmArena lsm;
+    qk::LsmArena lsm[qk::kLsmLanes];
+    qk::DevArena lsm_task, lsm_centre;    // descriptors and centring shifts of all jobs of a call
+    cudaStream_t lsm_stream[qk::kLsmLanes] = {};
+    cudaEvent_t lsm_fork = nullptr, lsm_join[qk::kLsmLanes] = {};
     qk::Plan plan;
     bool prepared = false;
     cudaGraphExec_t graph = nullptr;  // the prepared batch's launch sequence (qk_batch_prepare)

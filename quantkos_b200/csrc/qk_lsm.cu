@@ -774,17 +774,43 @@ void lsm_release(qk_handle *h) {
     for (cudaEvent_t e : h->lsm_events) cudaEventDestroy(e);
     h->lsm_events.clear();
     h->lsm_jobs = 0;
-    LsmArena &L = h->lsm;
-    L.slab_S.release();
-    L.slab_v.release();
-    L.cashflow.release();
-    L.block_sums.release();
-    L.coeffs.release();
-    L.task.release();
-    L.status.release();
+    for (int l = 0; l < kLsmLanes; ++l) {
+        LsmArena &L = h->lsm[l];
+        L.slab_S.release();
+        L.slab_v.release();
+        L.cashflow.release();
+        L.block_sums.release();
+        L.coeffs.release();
+        L.status.release();
+        if (h->lsm_stream[l]) cudaStreamDestroy(h->lsm_stream[l]);
+        if (h->lsm_join[l]) cudaEventDestroy(h->lsm_join[l]);
+        h->lsm_stream[l] = nullptr;
+        h->lsm_join[l] = nullptr;
+    }
+    if (h->lsm_fork) cudaEventDestroy(h->lsm_fork);
+    h->lsm_fork = nullptr;
+    h->lsm_task.release();
+    h->lsm_centre.release();
     h->h_lsm.release();
     h->d_lsm_moments.release();
 }
+
+namespace {
+
+// Streams and fork/join events of the LSM lanes (created on first use).
+qk_status lsm_lanes_ensure(qk_handle *h, int lanes) {
+    if (!h->lsm_fork && cudaEventCreateWithFlags(&h->lsm_fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(QK_ERR_CUDA, "LSM: cudaEventCreate failed");
+    for (int l = 0; l < lanes; ++l) {
+        if (!h->lsm_stream[l] && cudaStreamCreateWithFlags(&h->lsm_stream[l], cudaStreamNonBlocking) != cudaSuccess)
+            return fail(QK_ERR_CUDA, "LSM: cudaStreamCreate failed");
+        if (!h->lsm_join[l] && cudaEventCreateWithFlags(&h->lsm_join[l], cudaEventDisableTiming) != cudaSuccess)
+            return fail(QK_ERR_CUDA, "LSM: cudaEventCreate failed");
+    }
+    return QK_OK;
+}
+
+}  // namespace
 
 qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Moments> &moments) {
     (void)moments;
@@ -804,38 +830,58 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
     const int grid = h->sm_count * 2;
     const size_t nj = jobs.size();
     qk_status st;
-    // sizes
-    size_t max_slab = 0, max_cf = 0;
-    int max_dates = 1;
-    for (const Job &j : jobs) {
-        const int D = j.b.lsm_dates > 0 ? j.b.lsm_dates : j.b.n_steps;
-        const int64_t ld = (j.b.n_paths + 3) / 4 * 4;
-        const size_t esz = j.b.precision == QK_FP32 ? 4 : 8;
-        max_slab = std::max(max_slab, static_cast<size_t>(D) * ld * esz);
-        max_cf = std::max(max_cf, static_cast<size_t>(ld) * esz);
-        max_dates = std::max(max_dates, D);
+    // per-job working-set sizes
+    auto dates_of = [](const qk_contract &b) { return b.lsm_dates > 0 ? b.lsm_dates : b.n_steps; };
+    auto ld_of = [](const qk_contract &b) { return (b.n_paths + 3) / 4 * 4; };
+    auto esz_of = [](const qk_contract &b) { return static_cast<size_t>(b.precision == QK_FP32 ? 4 : 8); };
+    auto slab_of = [&](const Job &j) { return static_cast<size_t>(dates_of(j.b)) * ld_of(j.b) * esz_of(j.b); };
+    // Jobs go to the lanes longest first, each to the least loaded lane (by path-steps);
+    // a lane runs its jobs in order on its own stream and working set, sized for the
+    // largest of them, so the lanes together hold at most the sum over the jobs.
+    const int lanes = static_cast<int>(std::min<size_t>(kLsmLanes, std::max<size_t>(nj, 1)));
+    std::vector<size_t> order(nj);
+    for (size_t k = 0; k < nj; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+        return static_cast<double>(jobs[x].b.n_paths) * jobs[x].b.n_steps >
+               static_cast<double>(jobs[y].b.n_paths) * jobs[y].b.n_steps;
+    });
+    std::vector<int> lane_of(nj, 0);
+    std::vector<double> load(lanes, 0.0);
+    std::vector<size_t> lane_slab(lanes, 0), lane_cf(lanes, 0);
+    std::vector<int> lane_dates(lanes, 1);
+    std::vector<bool> lane_v(lanes, false);
+    for (size_t k : order) {
+        const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+        lane_of[k] = l;
+        load[l] += static_cast<double>(jobs[k].b.n_paths) * jobs[k].b.n_steps;
+        lane_slab[l] = std::max(lane_slab[l], slab_of(jobs[k]));
+        lane_cf[l] = std::max(lane_cf[l], static_cast<size_t>(ld_of(jobs[k].b)) * esz_of(jobs[k].b));
+        lane_dates[l] = std::max(lane_dates[l], dates_of(jobs[k].b));
+        lane_v[l] = lane_v[l] || jobs[k].b.lsm_basis == QK_LSM_POLY_SV;
     }
-    LsmArena &L = h->lsm;
-    if ((st = L.slab_S.ensure(max_slab)) != QK_OK) return st;
-    bool any_v = false;
-    for (const Job &j : jobs) any_v |= j.b.lsm_basis == QK_LSM_POLY_SV;
-    if (any_v && (st = L.slab_v.ensure(max_slab)) != QK_OK) return st;
-    if ((st = L.cashflow.ensure(max_cf)) != QK_OK) return st;
-    if ((st = L.block_sums.ensure(static_cast<size_t>(h->sm_count) * 4 * 32 * sizeof(double))) != QK_OK) return st;
-    if ((st = L.coeffs.ensure(static_cast<size_t>(max_dates) * kMaxCoef * sizeof(double) + 2 * max_dates * sizeof(double) * nj + 64)) != QK_OK) return st;
-    if ((st = L.status.ensure(static_cast<size_t>(max_dates) * sizeof(int) + 256)) != QK_OK) return st;
+    if ((st = lsm_lanes_ensure(h, lanes)) != QK_OK) return st;
+    for (int l = 0; l < lanes; ++l) {
+        LsmArena &L = h->lsm[l];
+        if ((st = L.slab_S.ensure(lane_slab[l])) != QK_OK) return st;
+        if (lane_v[l] && (st = L.slab_v.ensure(lane_slab[l])) != QK_OK) return st;
+        if ((st = L.cashflow.ensure(lane_cf[l])) != QK_OK) return st;
+        if ((st = L.block_sums.ensure(static_cast<size_t>(h->sm_count) * 4 * 32 * sizeof(double))) != QK_OK) return st;
+        if ((st = L.coeffs.ensure(static_cast<size_t>(lane_dates[l]) * kMaxCoef * sizeof(double) + 64)) != QK_OK)
+            return st;
+        if ((st = L.status.ensure(static_cast<size_t>(lane_dates[l]) * sizeof(int) + 256)) != QK_OK) return st;
+    }
     if ((st = lsm_events_ensure(h, 3 * nj)) != QK_OK) return st;
-    if ((st = L.task.ensure(nj * sizeof(TaskDev))) != QK_OK) return st;
+    if ((st = h->lsm_task.ensure(nj * sizeof(TaskDev))) != QK_OK) return st;
     if ((st = h->d_lsm_moments.ensure(nj * grid * sizeof(Moments))) != QK_OK) return st;
     if ((st = h->h_lsm.ensure(nj * grid * sizeof(Moments))) != QK_OK) return st;
-    // descriptors and per-date centring constants (one upload, blocking)
+    // descriptors and per-date centring constants of all jobs (one upload, blocking)
     std::vector<TaskDev> tasks(nj);
     std::vector<double> centres;
     std::vector<size_t> centre_off(nj);
     for (size_t k = 0; k < nj; ++k) {
         const qk_contract &b = jobs[k].b;
         tasks[k] = make_task(b, 1);
-        const int D = b.lsm_dates > 0 ? b.lsm_dates : b.n_steps;
+        const int D = dates_of(b);
         const int stride = b.n_steps / D;
         const double dt = b.T / b.n_steps;
         const double K = b.payoffs[0].strike;
@@ -847,25 +893,32 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
             centres.push_back(b.theta + (b.v0 - b.theta) * std::exp(-b.kappa * t));
         }
     }
-    double *d_coeffs = static_cast<double *>(L.coeffs.ptr);
-    double *d_centre = d_coeffs + static_cast<size_t>(max_dates) * kMaxCoef;
-    QK_CUDA_LSM(cudaMemcpy(L.task.ptr, tasks.data(), nj * sizeof(TaskDev), cudaMemcpyHostToDevice));
-    QK_CUDA_LSM(cudaMemcpy(d_centre, centres.data(), centres.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if ((st = h->lsm_centre.ensure(std::max<size_t>(centres.size(), 1) * sizeof(double))) != QK_OK) return st;
+    const double *d_centre = static_cast<const double *>(h->lsm_centre.ptr);
+    QK_CUDA_LSM(cudaMemcpy(h->lsm_task.ptr, tasks.data(), nj * sizeof(TaskDev), cudaMemcpyHostToDevice));
+    QK_CUDA_LSM(cudaMemcpy(h->lsm_centre.ptr, centres.data(), centres.size() * sizeof(double),
+                           cudaMemcpyHostToDevice));
+    // fork: the lanes start after the work already queued on the handle's stream
+    QK_CUDA_LSM(cudaEventRecord(h->lsm_fork, h->stream));
+    for (int l = 0; l < lanes; ++l) QK_CUDA_LSM(cudaStreamWaitEvent(h->lsm_stream[l], h->lsm_fork, 0));
     for (size_t k = 0; k < nj; ++k) {
         const qk_contract &b = jobs[k].b;
-        const int D = b.lsm_dates > 0 ? b.lsm_dates : b.n_steps;
+        const int l = lane_of[k];
+        LsmArena &L = h->lsm[l];
+        cudaStream_t s = h->lsm_stream[l];
+        const int D = dates_of(b);
         const int stride = b.n_steps / D;
-        const int64_t ld = (b.n_paths + 3) / 4 * 4;
+        const int64_t ld = ld_of(b);
         const int prec = b.precision;
         const bool use_v = b.lsm_basis == QK_LSM_POLY_SV;
         // forward: exercise-date slabs
-        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k], h->stream));
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k], s));
         // FP32: two paths per thread, stepped as pairs
-        QK_CUDA_LSM(launch_slab_paths(prec, b.model, b.scheme, b.seed, h->stream,
-                                      static_cast<const TaskDev *>(L.task.ptr) + k, 0, b.n_paths, stride, L.slab_S.ptr,
-                                      use_v ? L.slab_v.ptr : nullptr, ld, prec == QK_FP32 ? 2 : 1));
+        QK_CUDA_LSM(launch_slab_paths(prec, b.model, b.scheme, b.seed, s,
+                                      static_cast<const TaskDev *>(h->lsm_task.ptr) + k, 0, b.n_paths, stride,
+                                      L.slab_S.ptr, use_v ? L.slab_v.ptr : nullptr, ld, prec == QK_FP32 ? 2 : 1));
         h->lsm_launches++;
-        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 1], h->stream));
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 1], s));
         LsmArgs a;
         a.N = b.n_paths;
         a.ld = ld;
@@ -875,35 +928,39 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         a.disc = std::exp(-b.r * stride * (b.T / b.n_steps));
         Moments *bm = static_cast<Moments *>(h->d_lsm_moments.ptr) + k * grid;
         const double *cen = d_centre + centre_off[k];
+        double *d_coeffs = static_cast<double *>(L.coeffs.ptr);
         double *bs = static_cast<double *>(L.block_sums.ptr);
         int *fl = static_cast<int *>(L.status.ptr);
-        unsigned int *done = reinterpret_cast<unsigned int *>(static_cast<char *>(L.status.ptr) +
-                                                              ((static_cast<size_t>(max_dates) * sizeof(int) + 127) / 128) * 128);
+        unsigned int *done = reinterpret_cast<unsigned int *>(
+            static_cast<char *>(L.status.ptr) + ((static_cast<size_t>(lane_dates[l]) * sizeof(int) + 127) / 128) * 128);
         cudaError_t e;
         if (prec == QK_FP32) {
             if (use_v)
-                e = enqueue_backward<float, QK_LSM_POLY_SV>(h->stream, grid, h->sm_count, a, static_cast<const float *>(L.slab_S.ptr),
+                e = enqueue_backward<float, QK_LSM_POLY_SV>(s, grid, h->sm_count, a,
+                                                           static_cast<const float *>(L.slab_S.ptr),
                                                            static_cast<const float *>(L.slab_v.ptr),
-                                                           static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, done, bm,
-                                                           &h->lsm_launches);
+                                                           static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs,
+                                                           done, bm, &h->lsm_launches);
             else
-                e = enqueue_backward<float, QK_LSM_LAGUERRE3>(h->stream, grid, h->sm_count, a, static_cast<const float *>(L.slab_S.ptr),
-                                                             nullptr, static_cast<float *>(L.cashflow.ptr), d_coeffs, fl,
-                                                             cen, bs, done, bm, &h->lsm_launches);
+                e = enqueue_backward<float, QK_LSM_LAGUERRE3>(s, grid, h->sm_count, a,
+                                                             static_cast<const float *>(L.slab_S.ptr), nullptr,
+                                                             static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen,
+                                                             bs, done, bm, &h->lsm_launches);
         } else {
             if (use_v)
-                e = enqueue_backward<double, QK_LSM_POLY_SV>(h->stream, grid, h->sm_count, a, static_cast<const double *>(L.slab_S.ptr),
+                e = enqueue_backward<double, QK_LSM_POLY_SV>(s, grid, h->sm_count, a,
+                                                            static_cast<const double *>(L.slab_S.ptr),
                                                             static_cast<const double *>(L.slab_v.ptr),
-                                                            static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen, bs,
-                                                            done, bm, &h->lsm_launches);
+                                                            static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen,
+                                                            bs, done, bm, &h->lsm_launches);
             else
-                e = enqueue_backward<double, QK_LSM_LAGUERRE3>(h->stream, grid, h->sm_count, a,
+                e = enqueue_backward<double, QK_LSM_LAGUERRE3>(s, grid, h->sm_count, a,
                                                               static_cast<const double *>(L.slab_S.ptr), nullptr,
                                                               static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen,
                                                               bs, done, bm, &h->lsm_launches);
         }
         if (e != cudaSuccess) return fail(QK_ERR_CUDA, std::string("LSM launch: ") + cudaGetErrorString(e));
-        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 2], h->stream));
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_events[3 * k + 2], s));
         LsmTaskInfo info;
         info.contract = jobs[k].contract;
         info.role = jobs[k].role;
@@ -915,6 +972,11 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         info.eps = prec == QK_FP32 ? 1e-6 : 1e-12;
         plan.lsm_tasks.push_back(info);
         plan.lsm_path_steps += static_cast<double>(b.n_paths) * b.n_steps;
+    }
+    // join: the handle's stream continues once every lane is done
+    for (int l = 0; l < lanes; ++l) {
+        QK_CUDA_LSM(cudaEventRecord(h->lsm_join[l], h->lsm_stream[l]));
+        QK_CUDA_LSM(cudaStreamWaitEvent(h->stream, h->lsm_join[l], 0));
     }
     QK_CUDA_LSM(cudaMemcpyAsync(h->h_lsm.ptr, h->d_lsm_moments.ptr, nj * grid * sizeof(Moments),
                                 cudaMemcpyDeviceToHost, h->stream));

@@ -385,3 +385,22 @@ def test_edge_sizes_match_oracle(qk, handle, oracle):
     assert qk.price_batch([], None, handle) == []
     with pytest.raises(ValueError, match="N_Paths"):
         qk.price_batch([qk.make_contract(n_paths=2 ** 32)], None, handle)
+
+
+def test_lsm_jobs_on_concurrent_lanes_equal_alone(qk, handle):
+    """The American jobs of one call (contracts and their Greek bumps) run on several streams at
+    once, each with its own working set; every result equals the contract priced alone."""
+    cs = []
+    for i, (n, prec, basis) in enumerate([(20_000, qk.FP32, 1), (150_000, qk.FP32, 0), (60_000, qk.FP64, 1),
+                                          (8_192, qk.FP32, 1), (90_000, qk.FP64, 0)]):
+        cs.append(qk.make_contract(S0=100.0, v0=0.04, scheme=qk.ANDERSEN_QE if i % 2 == 0 else qk.EULER,
+                                   n_steps=50, n_paths=n, seed=7 + i, stream=i, precision=prec,
+                                   payoffs=[qk.payoff(qk.AMERICAN, qk.PUT, 95.0 + 3 * i)], lsm_basis=basis,
+                                   lsm_dates=0 if basis == 0 else 10))
+    g = qk.make_greeks(qk.GREEK_DELTA_GAMMA, bump_S_rel=0.01)
+    together = qk.price_batch(cs, g, handle)
+    for c, r in zip(cs, together):
+        alone = qk.price_batch([c], g, handle)[0]["legs"][0]
+        leg = r["legs"][0]
+        for f in ("price", "std_error", "prob_itm", "delta", "gamma"):
+            assert leg[f] == pytest.approx(alone[f], rel=1e-12, abs=1e-15), f
