@@ -293,8 +293,22 @@ struct BinHeader {
     double scale_factor = 1.0;
 };
 
+// Paths per stored batch of the .paths output, as MCConfig sizes the reference's
+// path batches (PathsMCBatchMem.hpp:330-390): Batch_Size > 0 fixed, -1 all paths,
+// 0 automatic from the device budget Max_VRAM_MB / (steps x element size), in
+// multiples of 32.  Pricing itself stores no paths.
+int64_t stored_batch_paths(const qk_config &cfg, const qk_contract &c) {
+    if (cfg.batch_size > 0) return std::min<int64_t>(cfg.batch_size, c.n_paths);
+    if (cfg.batch_size == -1) return c.n_paths;
+    const double esz = c.precision == QK_FP32 ? 4.0 : 8.0;
+    const int64_t fit = static_cast<int64_t>(static_cast<double>(cfg.max_vram_mb) * 1024.0 * 1024.0 /
+                                             (static_cast<double>(c.n_steps) * esz));
+    return std::min<int64_t>(c.n_paths, std::max<int64_t>(32, fit / 32 * 32));
+}
+
 template <class R>
-qk_status write_paths_file(qk_handle *h, const qk_contract &c, double dt, double scale, const std::string &path) {
+qk_status write_paths_file(qk_handle *h, const qk_contract &c, double dt, double scale, const std::string &path,
+                           int64_t chunk) {
     std::ofstream f(path, std::ios::out | std::ios::binary);
     if (!f.is_open()) return fail(QK_ERR_INVALID_ARG, "[BinWriter Error] Failed to open binary output file: " + path);
     BinHeader<R> hd;
@@ -303,7 +317,6 @@ qk_status write_paths_file(qk_handle *h, const qk_contract &c, double dt, double
     hd.dt = static_cast<R>(dt);
     hd.scale_factor = scale;
     f.write(reinterpret_cast<const char *>(&hd), sizeof(hd));
-    const int64_t chunk = std::max<int64_t>(1, (int64_t{1} << 26) / std::max(1, c.n_steps));
     std::vector<double> S;
     std::vector<R> row;
     for (int64_t first = 0; first < c.n_paths; first += chunk) {
@@ -480,8 +493,9 @@ qk_status qk_run_config(qk_handle *h, const qk_config *cfg, qk_result *out, doub
         const std::string path = (std::filesystem::path(c.out_dir) / c.paths_file).string();
         qk_timing keep;
         qk_last_timing(h, &keep);
-        qk_status st = (k.precision == QK_FP32) ? write_paths_file<float>(h, k, c.dt, scale, path)
-                                                : write_paths_file<double>(h, k, c.dt, scale, path);
+        const int64_t chunk = stored_batch_paths(c, k);
+        qk_status st = (k.precision == QK_FP32) ? write_paths_file<float>(h, k, c.dt, scale, path, chunk)
+                                                : write_paths_file<double>(h, k, c.dt, scale, path, chunk);
         h->timing = keep;
         if (st != QK_OK) return st;
     }

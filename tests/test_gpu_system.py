@@ -257,3 +257,19 @@ def test_autotuner_keeps_prices_and_reports_every_kind(qk, handle):
         handle.tune_set(1, 0, 3, 12, True)
     for r in report:  # back to the defaults for the tests that follow
         handle.tune_set(r["precision"], r["model"], r["scheme"], 24, False, 1)
+
+
+def test_paths_file_batching_keeps_the_file(qk, handle, tmp_path):
+    """MC.Batch_Size / MC.Max_VRAM_MB size the stored path batches of the .paths output with the
+    reference's rule (fixed, all, or from the device budget); the file is the same whatever the
+    batching, since every path's draws depend only on its index."""
+    blobs = []
+    for bs, vram in ((-1, 256), (64, 256), (0, 1)):
+        name = f"b{bs + 1}_{vram}.paths"
+        cfg = _cfg(qk, tmp_path, paths=name)
+        cfg.n_paths = 300
+        cfg.batch_size = bs
+        cfg.max_vram_mb = vram
+        qk.MCDispatcher(cfg, handle).launch_montecarlo()
+        blobs.append((tmp_path / name).read_bytes())
+    assert blobs[0] == blobs[1] == blobs[2]
