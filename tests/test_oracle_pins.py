@@ -208,3 +208,58 @@ def test_oracle_antithetic_pairs_black_scholes(oracle):
     assert abs(anti["price"] - bs) <= 3.0 * anti["std_error"]
     assert anti["std_error"] < 0.8 * plain["std_error"]
     assert 0.0 < anti["prob_itm"] < 1.0
+
+
+def _gil_pelaez_call(S0, K, T, r, q, v0, kappa, theta, sigma, rho, lam=0.0, mu_j=0.0, sigma_j=0.0):
+    """Independent check of the closed forms: the Heston characteristic function of log S_T in the
+    Albrecher et al. (2007) form, times the lognormal-jump factor for Bates (log-jumps N(mu_j,
+    sigma_j^2) at rate lam, drift compensated), inverted by Gil-Pelaez with adaptive quadrature
+    on [0, inf)."""
+    import cmath
+
+    from scipy.integrate import quad
+    kbar = math.exp(mu_j + 0.5 * sigma_j * sigma_j) - 1.0
+
+    def phi(u):
+        iu = 1j * u
+        b = kappa - rho * sigma * iu
+        d = cmath.sqrt(b * b + sigma * sigma * (iu + u * u))
+        g = (b - d) / (b + d)
+        e = cmath.exp(-d * T)
+        c = (kappa * theta / sigma ** 2) * ((b - d) * T - 2.0 * cmath.log((1.0 - g * e) / (1.0 - g)))
+        dd = (v0 / sigma ** 2) * (b - d) * (1.0 - e) / (1.0 - g * e)
+        jump = lam * T * (cmath.exp(iu * mu_j - 0.5 * sigma_j ** 2 * u * u) - 1.0) - iu * lam * kbar * T
+        return cmath.exp(iu * (math.log(S0) + (r - q) * T) + c + dd + jump)
+
+    lk = math.log(K)
+    phi_mi = phi(-1j).real
+    f2 = lambda u: (cmath.exp(-1j * u * lk) * phi(u) / (1j * u)).real  # noqa: E731
+    f1 = lambda u: (cmath.exp(-1j * u * lk) * phi(u - 1j) / (1j * u * phi_mi)).real  # noqa: E731
+    p2 = 0.5 + quad(f2, 0.0, math.inf, limit=500, epsabs=1e-12)[0] / math.pi
+    p1 = 0.5 + quad(f1, 0.0, math.inf, limit=500, epsabs=1e-12)[0] / math.pi
+    return S0 * math.exp(-q * T) * p1 - K * math.exp(-r * T) * p2
+
+
+@pytest.mark.parametrize("case", [
+    dict(S0=100.0, K=100.0, T=1.0, r=0.03, q=0.0, v0=0.04, kappa=2.0, theta=0.04, sigma=0.3, rho=-0.7),
+    dict(S0=100.0, K=120.0, T=0.5, r=0.05, q=0.02, v0=0.09, kappa=1.0, theta=0.06, sigma=0.6, rho=-0.3),
+    dict(S0=100.0, K=90.0, T=2.0, r=0.01, q=0.0, v0=0.02, kappa=4.0, theta=0.05, sigma=0.2, rho=-0.9),
+    dict(S0=100.0, K=100.0, T=1.0, r=0.03, q=0.0, v0=0.04, kappa=2.0, theta=0.04, sigma=0.3, rho=-0.7,
+         lam=0.1, mu_j=-0.05, sigma_j=0.10),
+    dict(S0=100.0, K=110.0, T=0.75, r=0.02, q=0.01, v0=0.05, kappa=1.5, theta=0.05, sigma=0.4, rho=-0.5,
+         lam=0.5, mu_j=-0.15, sigma_j=0.2),
+])
+def test_oracle_closed_forms_vs_adaptive_quadrature(oracle, case):
+    make_contract = _make()
+    from quantkos_b200 import _lib as L
+    bates = "lam" in case
+    k = make_contract(S0=case["S0"], v0=case["v0"], r=case["r"], q=case["q"], kappa=case["kappa"],
+                      theta=case["theta"], sigma=case["sigma"], rho=case["rho"], T=case["T"],
+                      model=L.BATES if bates else L.HESTON, lambda_j=case.get("lam", 0.0),
+                      mu_j=case.get("mu_j", 0.0), sigma_j=case.get("sigma_j", 0.0),
+                      payoffs=[L.Payoff(0, 0, case["K"], 0.0)])
+    want = _gil_pelaez_call(case["S0"], case["K"], case["T"], case["r"], case["q"], case["v0"], case["kappa"],
+                            case["theta"], case["sigma"], case["rho"], case.get("lam", 0.0),
+                            case.get("mu_j", 0.0), case.get("sigma_j", 0.0))
+    got = oracle.exact_call(2 if bates else 1, k, 0.0 if bates else 200.0)
+    assert abs(got - want) < 1e-8, (got, want)
