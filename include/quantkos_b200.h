@@ -223,6 +223,8 @@ typedef struct qk_tune_report {
  * Prices do not depend on the shape beyond the last bits of the moment merge. */
 qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g, int32_t reps,
                       qk_tune_report *out);
+/* Restores the default shape of every kind. */
+qk_status qk_tune_reset(qk_handle *h);
 /* Sets one kind's shape by hand (for example a stored autotuner result). */
 qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t scheme, int32_t tiles_per_warp,
                       int32_t guided_tail, int32_t paths_per_lane);

@@ -130,6 +130,7 @@ SIGNATURES = {
     "qk_last_timing": (C.c_int, [_VP, _P(Timing)]),
     "qk_autotune": (C.c_int, [_VP, _P(Contract), C.c_int32, _P(Greeks), C.c_int32, _P(TuneReport)]),
     "qk_tune_set": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "qk_tune_reset": (C.c_int, [_VP]),
     "qk_measure_sfu": (C.c_int, [_VP, _P(C.c_double)]),
     "qk_validate": (C.c_int, [_P(Contract), _P(Greeks)]),
     "qk_price_plain": (C.c_int, [_VP, _P(Contract), _P(Greeks), _P(Result)]),

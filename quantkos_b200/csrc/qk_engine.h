@@ -81,6 +81,7 @@ struct qk_handle {
     cudaGraphExec_t graph = nullptr;  // the prepared batch's launch sequence (qk_batch_prepare)
     int64_t graph_launches = 0;
     // launch shape per kernel kind [precision][model][scheme] (autotuner)
+    // defaults (qk_tune_reset): 24 tiles per warp slot, one path per lane, no guided tail
     int tune_tpw[2][2][3] = {{{24, 24, 24}, {24, 24, 24}}, {{24, 24, 24}, {24, 24, 24}}};
     int tune_tail[2][2][3] = {};
     int tune_lanes[2][2][3] = {{{1, 1, 1}, {1, 1, 1}}, {{1, 1, 1}, {1, 1, 1}}};  // paths per lane: 1 or 2

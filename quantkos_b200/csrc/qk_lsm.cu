@@ -525,9 +525,10 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     int64_t chunk = blockIdx.x;
     if (chunk < n_chunks) issue(chunk, 0, true, false);
     pdl_wait_preceding();
-    double cu[NB];
-#pragma unroll
-    for (int i = 0; i < NB; ++i) cu[i] = init ? 0.0 : coeffs[d_upd * kMaxCoef + i];
+    // this date's coefficients, read by every thread from shared memory (broadcast);
+    // the loop's first barrier orders these stores before any read
+    __shared__ double cu[kMaxCoef];
+    if (threadIdx.x < NB) cu[threadIdx.x] = init ? 0.0 : coeffs[d_upd * kMaxCoef + threadIdx.x];
     if (chunk < n_chunks) issue(chunk, 0, false, true);
     cp_async_commit();
     for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {

@@ -354,11 +354,11 @@ __device__ __forceinline__ void simulate_dispatch(const TaskDev &t, const StepCo
 }
 
 // ----------------------------------------------------------------------------
-// Fused pricing kernel.  Persistent: each block pops queue slots from a device
+// Fused pricing kernel.  Persistent: each warp pops queue slots from a device
 // cursor; slot q belongs to the task whose tile range [tile_begin, tile_begin +
 // n_tiles) holds it (binary search over the task prefix, tasks ordered by the
-// host's schedule).  A tile is ppt rounds of one path per thread; every
-// requested payoff leg is evaluated in registers and folded into per-warp FP64
+// host's schedule).  A tile is a number of rounds in which every lane simulates
+// one lane unit (a path, an antithetic pair or two paths); every requested payoff leg is evaluated in registers and folded into per-warp FP64
 // moments (n, mean, M2, #ITM), then into one record per tile and leg.  The
 // reference writes payoffs to memory and reduces them in two more passes
 // (OptionPricer.hpp:123-193); here nothing per path leaves registers.
@@ -621,7 +621,8 @@ __global__ void __launch_bounds__(128) merge_task_chunks_kernel(const TaskDev *_
     }
 }
 
-// Exercise-date slabs (LSM) / full path dump: one path per thread, S (and v)
+// Exercise-date slabs (LSM) / full path dump: one path per thread (a two-path
+// variant follows), S (and v)
 // after every `stride`-th step stored as SoA rows slab[date][path] (coalesced:
 // consecutive threads write consecutive columns).  Specialised per kind, with the
 // Philox round keys in the kernel parameters.

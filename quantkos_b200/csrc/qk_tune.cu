@@ -28,11 +28,24 @@ namespace {
 constexpr int kTilesPerWarp[] = {4, 8, 12, 24, 48};
 constexpr int kTails[] = {0, 1};
 constexpr int kLanes[] = {1, 2};
-constexpr int kDefaultTpw = 24;  // the handle's defaults (qk_engine.h)
-constexpr int kDefaultTail = 0;
-constexpr int kDefaultLanes = 1;
+// The handle's default shape of a kind (the initial values in qk_engine.h).
+void default_shape(int precision, int &tpw, int &tail, int &lanes) {
+    (void)precision;
+    tpw = 24;
+    tail = 0;
+    lanes = 1;
+}
 
 }  // namespace
+
+extern "C" qk_status qk_tune_reset(qk_handle *h) {
+    if (!h) return qk::fail(QK_ERR_INVALID_ARG, "qk_tune_reset: NULL handle");
+    for (int pr = 0; pr < 2; ++pr)
+        for (int md = 0; md < 2; ++md)
+            for (int sc = 0; sc < 3; ++sc)
+                default_shape(pr, h->tune_tpw[pr][md][sc], h->tune_tail[pr][md][sc], h->tune_lanes[pr][md][sc]);
+    return QK_OK;
+}
 
 extern "C" qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t scheme,
                                  int32_t tiles_per_warp, int32_t guided_tail, int32_t paths_per_lane) {
@@ -77,7 +90,9 @@ extern "C" qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, 
         }
         std::vector<qk_result> res(sub.size());
         double best = std::numeric_limits<double>::infinity(), dflt = 0.0;
-        int best_tpw = kDefaultTpw, best_tail = kDefaultTail, best_lanes = kDefaultLanes;
+        int dflt_tpw, dflt_tail, dflt_lanes;
+        default_shape(pr, dflt_tpw, dflt_tail, dflt_lanes);
+        int best_tpw = dflt_tpw, best_tail = dflt_tail, best_lanes = dflt_lanes;
         for (int lanes : kLanes)
             for (int tpw : kTilesPerWarp)
                 for (int tail : kTails) {
@@ -89,14 +104,13 @@ extern "C" qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, 
                         const qk_status s = qk::price_contracts(h, sub.data(), static_cast<int32_t>(sub.size()),
                                                                 gsub.data(), res.data(), false);
                         if (s != QK_OK) {
-                            h->tune_tpw[pr][md][sc] = kDefaultTpw;
-                            h->tune_tail[pr][md][sc] = kDefaultTail;
-                            h->tune_lanes[pr][md][sc] = kDefaultLanes;
+                            default_shape(pr, h->tune_tpw[pr][md][sc], h->tune_tail[pr][md][sc],
+                                          h->tune_lanes[pr][md][sc]);
                             return s;
                         }
                         if (r > 0) ms = std::min(ms, h->timing.device_ms);
                     }
-                    if (tpw == kDefaultTpw && tail == kDefaultTail && lanes == kDefaultLanes) dflt = ms;
+                    if (tpw == dflt_tpw && tail == dflt_tail && lanes == dflt_lanes) dflt = ms;
                     if (ms < best) {
                         best = ms;
                         best_tpw = tpw;

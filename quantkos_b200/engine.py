@@ -110,6 +110,10 @@ class Handle:
                  "paths_per_lane": rep.paths_per_lane[k],
                  "best_ms": rep.best_ms[k], "default_ms": rep.default_ms[k]} for k in range(rep.n_kinds)]
 
+    def tune_reset(self) -> None:
+        """Back to the default launch shape of every kernel kind."""
+        check(L.lib().qk_tune_reset(self.ptr), "qk_tune_reset")
+
     def tune_set(self, precision: int, model: int, scheme: int, tiles_per_warp: int, guided_tail: bool,
                  paths_per_lane: int = 1) -> None:
         check(L.lib().qk_tune_set(self.ptr, precision, model, scheme, tiles_per_warp, int(guided_tail),

@@ -357,7 +357,7 @@ def test_lane_modes_simulate_the_same_paths(qk, handle, model, scheme):
             handle.tune_set(qk.FP32, model, scheme, 24, False, lanes)
             out.append(qk.price_batch([c], None, handle)[0]["legs"])
     finally:
-        handle.tune_set(qk.FP32, model, scheme, 24, False, 1)
+        handle.tune_reset()
     for a, b in zip(out[0], out[1]):
         assert a["price"] == pytest.approx(b["price"], rel=1e-12, abs=1e-15)
         assert a["std_error"] == pytest.approx(b["std_error"], rel=1e-9)

@@ -255,8 +255,7 @@ def test_autotuner_keeps_prices_and_reports_every_kind(qk, handle):
         assert a["legs"][0]["std_error"] == pytest.approx(b["legs"][0]["std_error"], rel=1e-9)
     with pytest.raises(ValueError):
         handle.tune_set(1, 0, 3, 12, True)
-    for r in report:  # back to the defaults for the tests that follow
-        handle.tune_set(r["precision"], r["model"], r["scheme"], 24, False, 1)
+    handle.tune_reset()  # back to the defaults for the tests that follow
 
 
 def test_paths_file_batching_keeps_the_file(qk, handle, tmp_path):
