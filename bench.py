@@ -533,7 +533,10 @@ def main() -> None:
                  "std_error_fp64": [leg["std_error"] for leg in r64["legs"]],
                  "std_error_fp32": [leg["std_error"] for leg in res[0]["legs"]],
                  "price_fp64": [leg["price"] for leg in r64["legs"]],
-                 "price_fp32": [leg["price"] for leg in res[0]["legs"]]}
+                 "price_fp32": [leg["price"] for leg in res[0]["legs"]],
+                 # the FP32 batched price minus the FP64 drop-in price, in units of the FP64 standard error
+                 "fp32_minus_fp64_in_se": [(a["price"] - b["price"]) / b["std_error"] if b["std_error"] > 0 else 0.0
+                                           for a, b in zip(res[0]["legs"], r64["legs"])]}
 
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"

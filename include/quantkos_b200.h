@@ -10,7 +10,7 @@
  * bindings a maintainer adds.
  *
  * Threading: a handle is used by one host thread at a time, except
- * qk_serve_submit / qk_serve_poll, which are thread-safe.
+ * qk_serve_submit / qk_serve_poll / qk_serve_cancel, which are thread-safe.
  */
 #ifndef QUANTKOS_B200_H
 #define QUANTKOS_B200_H
@@ -36,7 +36,8 @@ typedef enum qk_status {
     QK_ERR_CAPACITY = 6,      /* request larger than the admission budget */
     QK_ERR_NO_DEVICE = 7,
     QK_ERR_PARSE = 8,         /* runtime_error "Config Error: ..." (src/IO/ConfigParser.cpp:36-294) */
-    QK_ERR_STATE = 9          /* call out of order (e.g. poll of an unknown ticket) */
+    QK_ERR_STATE = 9,         /* call out of order (e.g. poll of an unknown ticket) */
+    QK_ERR_CANCELLED = 10     /* the request was cancelled before it was admitted (qk_serve_cancel) */
 } qk_status;
 
 /* ---------------------------------------------------------------- enums
@@ -324,6 +325,10 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
 qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g, int64_t *ticket);
 /* done = 1 and *out filled once the ticket finished; wait_ms bounds the wait (0 = poll). */
 qk_status qk_serve_poll(qk_server *s, int64_t ticket, int32_t wait_ms, int32_t *done, qk_result *out);
+/* Withdraws a request that is still waiting for admission: *cancelled = 1 and its
+ * poll then reports QK_ERR_CANCELLED.  A request already admitted to a batch runs to
+ * completion (*cancelled = 0).  Thread-safe. */
+qk_status qk_serve_cancel(qk_server *s, int64_t ticket, int32_t *cancelled);
 qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out);
 qk_status qk_serve_stop(qk_server *s);
 

@@ -24,6 +24,7 @@ QK_ERR_CAPACITY = 6
 QK_ERR_NO_DEVICE = 7
 QK_ERR_PARSE = 8
 QK_ERR_STATE = 9
+QK_ERR_CANCELLED = 10
 
 # enums (quantkos::Implemented order)
 HESTON, BATES = 0, 1
@@ -151,6 +152,7 @@ SIGNATURES = {
     "qk_serve_start": (C.c_int, [_VP, C.c_int64, C.c_int32, _P(_VP)]),
     "qk_serve_submit": (C.c_int, [_VP, _P(Contract), _P(Greeks), _P(C.c_int64)]),
     "qk_serve_poll": (C.c_int, [_VP, C.c_int64, C.c_int32, _P(C.c_int32), _P(Result)]),
+    "qk_serve_cancel": (C.c_int, [_VP, C.c_int64, _P(C.c_int32)]),
     "qk_serve_stats_get": (C.c_int, [_VP, _P(ServeStats)]),
     "qk_serve_stop": (C.c_int, [_VP]),
 }

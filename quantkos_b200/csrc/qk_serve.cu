@@ -18,6 +18,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -54,7 +55,9 @@ size_t footprint(const qk_contract &c, const qk_greeks &g) {
         const size_t D = c.lsm_dates > 0 ? c.lsm_dates : c.n_steps;
         const size_t ld = (static_cast<size_t>(c.n_paths) + 3) / 4 * 4;
         const size_t slabs = c.lsm_basis == QK_LSM_POLY_SV ? 2 : 1;
-        bytes += D * ld * esz * slabs + ld * esz;  // slabs are reused across the bumps of one request
+        // the bumps of one request run on up to kLsmLanes streams at once, each with its own slabs
+        const size_t concurrent = std::min<size_t>(roles, qk::kLsmLanes);
+        bytes += concurrent * (D * ld * esz * slabs + ld * esz);
     } else {
         const size_t tiles = (static_cast<size_t>(c.n_paths) + qk::kWarpTilePaths - 1) / qk::kWarpTilePaths;
         bytes += roles * tiles * c.n_payoffs * sizeof(qk::Moments);
@@ -209,7 +212,30 @@ qk_status qk_serve_poll(qk_server *s, int64_t ticket, int32_t wait_ms, int32_t *
     if (out) *out = it->second.r;
     const qk_status st = it->second.status;
     s->done.erase(it);
+    if (st == QK_ERR_CANCELLED) return qk::fail(st, "qk_serve_poll: request cancelled before admission");
+    if (st != QK_OK) return qk::fail(st, "qk_serve_poll: request failed while pricing, status " + std::to_string(st));
     return st;
+}
+
+qk_status qk_serve_cancel(qk_server *s, int64_t ticket, int32_t *cancelled) {
+    if (!s || !cancelled) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    *cancelled = 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (ticket <= 0 || ticket >= s->next_ticket) return qk::fail(QK_ERR_STATE, "unknown ticket");
+        auto it = std::find_if(s->queue.begin(), s->queue.end(), [&](const Request &r) { return r.ticket == ticket; });
+        if (it == s->queue.end()) return QK_OK;  // admitted already (or finished): it completes
+        s->queue.erase(it);
+        Finished f;
+        std::memset(&f.r, 0, sizeof(f.r));
+        f.r.status = QK_ERR_CANCELLED;
+        f.status = QK_ERR_CANCELLED;
+        f.latency_ms = 0.0;
+        s->done[ticket] = f;
+        *cancelled = 1;
+    }
+    s->cv_done.notify_all();
+    return QK_OK;
 }
 
 qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out) {

@@ -375,6 +375,12 @@ class Server:
         check(L.lib().qk_serve_poll(self._s, ticket, wait_ms, C.byref(done), C.byref(out)), "qk_serve_poll")
         return result_to_dict(out) if done.value else None
 
+    def cancel(self, ticket: int) -> bool:
+        """Withdraw a request still waiting for admission (its poll then raises QK_ERR_CANCELLED)."""
+        c = C.c_int32()
+        check(L.lib().qk_serve_cancel(self._s, ticket, C.byref(c)), "qk_serve_cancel")
+        return bool(c.value)
+
     def stats(self) -> dict:
         s = L.ServeStats()
         check(L.lib().qk_serve_stats_get(self._s, C.byref(s)))

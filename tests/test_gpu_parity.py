@@ -180,7 +180,7 @@ def test_lsm_fp32_close_to_fp64(qk, handle):
     assert p64["price"] > euro["price"]  # early-exercise premium of the put
 
 
-@pytest.mark.parametrize("model,scheme", [(0, 2), (1, 2), (0, 1), (1, 0)])
+@pytest.mark.parametrize("model,scheme", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)])
 def test_prices_vs_closed_form(qk, handle, oracle, model, scheme):
     """European call within 3 SE of the Gil-Pelaez price (HestonTest/BatesTest parameters, 512 steps)."""
     d = load("reference_tests.json")["heston_call_rouah_p28"]["params"]
@@ -189,6 +189,18 @@ def test_prices_vs_closed_form(qk, handle, oracle, model, scheme):
                          mu_j=-0.15, sigma_j=0.11, T=0.5, n_steps=512, n_paths=1_000_000, seed=2026,
                          precision=qk.FP32, payoffs=[qk.payoff(0, 0, 100.0)])
     exact = oracle.exact_call(2 if model else 1, k)
+    got = qk.price_batch([k], None, handle)[0]["legs"][0]
+    assert abs(got["price"] - exact) <= 3.0 * got["std_error"], (got, exact)
+
+
+@pytest.mark.parametrize("model,scheme", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)])
+def test_black_scholes_limit(qk, handle, oracle, model, scheme):
+    """include/tests/Options/BlackScholesTest.hpp: kappa = theta = sigma = 0 (and no jumps) leaves
+    the variance at v0, so every model and scheme prices the Black-Scholes call within 3 SE."""
+    k = qk.make_contract(S0=100.0, v0=0.04, r=0.04, q=0.0, model=model, scheme=scheme, kappa=0.0, theta=0.0,
+                         sigma=0.0, rho=0.0, lambda_j=0.0, T=1.0, n_steps=64, n_paths=1_000_000, seed=31,
+                         precision=qk.FP32, payoffs=[qk.payoff(qk.EUROPEAN, qk.CALL, 100.0)])
+    exact = oracle.exact_call(0, k)
     got = qk.price_batch([k], None, handle)[0]["legs"][0]
     assert abs(got["price"] - exact) <= 3.0 * got["std_error"], (got, exact)
 

@@ -272,3 +272,28 @@ def test_paths_file_batching_keeps_the_file(qk, handle, tmp_path):
         qk.MCDispatcher(cfg, handle).launch_montecarlo()
         blobs.append((tmp_path / name).read_bytes())
     assert blobs[0] == blobs[1] == blobs[2]
+
+
+def test_server_cancels_waiting_requests(qk, handle):
+    """A request still waiting for admission can be withdrawn: its poll reports the cancellation,
+    the requests around it complete, an admitted or finished request is not cancelled, and an
+    unknown ticket is an error."""
+    from quantkos_b200 import _lib as L
+    from quantkos_b200 import workloads as W
+    long_job = W.bates_qe_five_payoffs(n_paths=16_777_216)  # keeps both lanes busy for tens of ms
+    small = qk.make_contract(n_paths=10_000, n_steps=10)
+    with qk.Server(handle, 0, 1) as srv:  # one request per batch
+        t_busy = [srv.submit(long_job) for _ in range(2)]
+        t_keep = srv.submit(small)
+        t_drop = srv.submit(small)
+        assert srv.cancel(t_drop)
+        with pytest.raises(RuntimeError) as err:
+            while srv.poll(t_drop, 1000) is None:
+                pass
+        assert err.value.status == L.QK_ERR_CANCELLED
+        for t in t_busy + [t_keep]:
+            while srv.poll(t, 1000) is None:
+                pass
+        assert not srv.cancel(t_keep)
+        with pytest.raises(RuntimeError, match="unknown ticket"):
+            srv.cancel(10_000)
