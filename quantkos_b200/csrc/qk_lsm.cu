@@ -168,6 +168,49 @@ __device__ __forceinline__ void accumulate(double *acc, R S, R v, R K, double in
     }
 }
 
+// FP32 slab with the 6-term basis: the per-path work (centred point, monomials,
+// continuation) in FP32 on path pairs (sm_100 paired FP32 instructions), without
+// branches — a path out of the money contributes the point (0, 0) with weight 0 —
+// and the 21 sums kept in FP32 for kF32Flush chunk rounds (eight paths per
+// accumulator) before the thread adds them to its FP64 sums.  An FP32 partial over
+// eight paths carries a relative rounding error of order 1e-7 — the size of the FP32
+// slab values' own rounding — and partials round independently, so the FP64 totals
+// over N paths stay accurate to far below the Monte Carlo error; the block and grid
+// reductions and the solve remain FP64.
+constexpr int kF32Flush = 4;
+
+__device__ __forceinline__ float continuation_f32(const float *c, float x, float w) {
+    return fmaf(w, fmaf(x, c[5], c[4]), fmaf(x, fmaf(x, fmaf(x, c[3], c[2]), c[1]), c[0]));
+}
+
+// Same 21 sums as accumulate<R, QK_LSM_POLY_SV>, in FP32 on two paths; one = path
+// weight (1 in the money, 0 otherwise, with x = w = y = 0).
+__device__ __forceinline__ void accumulate_f32x2(float2 *acc, float2 x, float2 w, float2 y, float2 one) {
+    const float2 x2 = __fmul2_rn(x, x), x3 = __fmul2_rn(x2, x), ww = __fmul2_rn(w, w);
+    const float2 wx = __fmul2_rn(w, x), wx2 = __fmul2_rn(w, x2);
+    acc[0] = __fadd2_rn(acc[0], one);
+    acc[1] = __fadd2_rn(acc[1], x);
+    acc[2] = __fadd2_rn(acc[2], x2);
+    acc[3] = __fadd2_rn(acc[3], x3);
+    acc[4] = __ffma2_rn(x2, x2, acc[4]);
+    acc[5] = __ffma2_rn(x2, x3, acc[5]);
+    acc[6] = __ffma2_rn(x3, x3, acc[6]);
+    acc[7] = __fadd2_rn(acc[7], w);
+    acc[8] = __fadd2_rn(acc[8], wx);
+    acc[9] = __fadd2_rn(acc[9], wx2);
+    acc[10] = __ffma2_rn(wx2, x, acc[10]);
+    acc[11] = __ffma2_rn(wx2, x2, acc[11]);
+    acc[12] = __fadd2_rn(acc[12], ww);
+    acc[13] = __ffma2_rn(ww, x, acc[13]);
+    acc[14] = __ffma2_rn(ww, x2, acc[14]);
+    acc[15] = __fadd2_rn(acc[15], y);
+    acc[16] = __ffma2_rn(y, x, acc[16]);
+    acc[17] = __ffma2_rn(y, x2, acc[17]);
+    acc[18] = __ffma2_rn(y, x3, acc[18]);
+    acc[19] = __ffma2_rn(y, w, acc[19]);
+    acc[20] = __ffma2_rn(y, wx, acc[20]);
+}
+
 // The solver's input: upper Gram (row-major), right-hand side, count.
 template <int BASIS>
 __device__ __forceinline__ void expand_sums(const double *acc, double *sums) {
@@ -402,7 +445,10 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // its writes are visible (immediately when there is no programmatic dependency).
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait_preceding() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_pending() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 constexpr int kLsmChunk = 4 * kLsmBlock;  // paths per staged chunk: four per thread
 
@@ -438,9 +484,21 @@ struct StageLayout {
     static constexpr int kSu = 0, kCf = 1, kSg = 2, kVu = 3, kVg = 4;
 };
 
+// Chunks in flight per block: with two resident blocks per SM, four FP32 stages keep
+// about 48 KB of slab rows per SM outstanding (enough to cover HBM latency at full
+// bandwidth); FP64 rows are twice the size, so two stages hold a comparable amount.
+template <class R, int BASIS>
+constexpr bool lsm_f32_poly() {
+    return sizeof(R) == 4 && BASIS == QK_LSM_POLY_SV;
+}
+template <class R>
+constexpr int lsm_stages() {
+    return sizeof(R) == 4 ? 4 : 2;
+}
+
 template <class R, int BASIS>
 constexpr size_t lsm_sweep_smem() {
-    return 2 * StageLayout<BASIS>::kArrays * kLsmChunk * sizeof(R);
+    return lsm_stages<R>() * StageLayout<BASIS>::kArrays * kLsmChunk * sizeof(R);
 }
 
 // Backward sweep over one date pair.  init: cash flows start as the payoff at
@@ -468,6 +526,7 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     constexpr int NSUM = Sums<NB>::NSUM;
     constexpr int NACC = AccTraits<BASIS>::N;
     constexpr bool use_v = BASIS == QK_LSM_POLY_SV;
+    constexpr bool kF32 = lsm_f32_poly<R, BASIS>();  // FP32 paired per-path work
     using L = StageLayout<BASIS>;
     extern __shared__ __align__(16) unsigned char lsm_smem[];
     R *stage = reinterpret_cast<R *>(lsm_smem);
@@ -480,6 +539,19 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
     double acc[NACC];
 #pragma unroll
     for (int j = 0; j < NACC; ++j) acc[j] = 0.0;
+    float2 acc2[kF32 ? NACC : 1];
+#pragma unroll
+    for (int j = 0; j < (kF32 ? NACC : 1); ++j) acc2[j] = make_float2(0.0f, 0.0f);
+    // adds this thread's FP32 partials to its FP64 sums
+    auto flush = [&]() {
+        if constexpr (kF32) {
+#pragma unroll
+            for (int j = 0; j < NACC; ++j) {
+                acc[j] += static_cast<double>(acc2[j].x) + static_cast<double>(acc2[j].y);
+                acc2[j] = make_float2(0.0f, 0.0f);
+            }
+        }
+    };
     double cxu = 0.0, cvu = 0.0, cxg = 0.0, cvg = 0.0;
     if (!init) {
         cxu = centre[2 * d_upd];
@@ -489,6 +561,9 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
         cxg = centre[2 * d_gram];
         cvg = centre[2 * d_gram + 1];
     }
+    const float inv_Kf = static_cast<float>(inv_K);
+    const float cxuf = static_cast<float>(cxu), cvuf = static_cast<float>(cvu);
+    const float cxgf = static_cast<float>(cxg), cvgf = static_cast<float>(cvg);
     const R *Su = slab_S + static_cast<int64_t>(d_upd) * a.ld;
     const R *Vu = use_v ? slab_v + static_cast<int64_t>(d_upd) * a.ld : nullptr;
     const R *Sg = slab_S + static_cast<int64_t>(gram ? d_gram : 0) * a.ld;
@@ -520,27 +595,83 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
         }
     };
 
-    // The first chunk's slab rows do not depend on the previous date: fetch them
+    // The first chunks' slab rows do not depend on the previous date: fetch them
     // before waiting for it; the cash flows and this date's coefficients after.
+    // Chunk k of this block (blockIdx.x + k * gridDim.x) goes to stage k mod ST.
+    // Commit groups: the first holds the rows of chunks 0 .. ST-2 and the cash flows
+    // of chunk 0, group g (1 <= g <= ST-2) the cash flows of chunk g, and loop
+    // iteration k commits chunk k + ST - 1 (possibly an empty group), so chunk k has
+    // landed once at most ST - 2 groups are pending.
+    constexpr int ST = lsm_stages<R>();
     int64_t chunk = blockIdx.x;
-    if (chunk < n_chunks) issue(chunk, 0, true, false);
+    for (int s = 0; s < ST - 1; ++s) {
+        const int64_t c = chunk + static_cast<int64_t>(s) * gridDim.x;
+        if (c < n_chunks) issue(c, s, true, false);
+    }
     pdl_wait_preceding();
     // this date's coefficients, read by every thread from shared memory (broadcast);
     // the loop's first barrier orders these stores before any read
     __shared__ double cu[kMaxCoef];
-    if (threadIdx.x < NB) cu[threadIdx.x] = init ? 0.0 : coeffs[d_upd * kMaxCoef + threadIdx.x];
-    if (chunk < n_chunks) issue(chunk, 0, false, true);
-    cp_async_commit();
-    for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {
-        const int64_t next = chunk + gridDim.x;
-        if (next < n_chunks) issue(next, (k + 1) & 1, true, true);
+    __shared__ float cuf[kMaxCoef];
+    if (threadIdx.x < NB) {
+        const double c = init ? 0.0 : coeffs[d_upd * kMaxCoef + threadIdx.x];
+        cu[threadIdx.x] = c;
+        cuf[threadIdx.x] = static_cast<float>(c);
+    }
+    for (int s = 0; s < ST - 1; ++s) {
+        const int64_t c = chunk + static_cast<int64_t>(s) * gridDim.x;
+        if (c < n_chunks) issue(c, s, false, true);
         cp_async_commit();
-        cp_async_wait_all_but_one();  // this thread's copies of `chunk` have landed
-        __syncthreads();              // ... and every other thread's
-        const R *base = stage + static_cast<size_t>(k & 1) * L::kArrays * kLsmChunk;
+    }
+    for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {
+        cp_async_wait_pending<ST - 2>();  // this thread's copies of `chunk` have landed
+        __syncthreads();  // ... and every other thread's; all threads are done with chunk k - 1
+        // refill the stage chunk k - 1 used, overlapping this chunk's arithmetic
+        const int64_t ahead = chunk + static_cast<int64_t>(ST - 1) * gridDim.x;
+        if (ahead < n_chunks) issue(ahead, (k + ST - 1) % ST, true, true);
+        cp_async_commit();
+        const R *base = stage + static_cast<size_t>(k % ST) * L::kArrays * kLsmChunk;
         // four consecutive paths per thread: 16-byte shared loads, no bank conflicts
         const int j0 = 4 * threadIdx.x;
         const int64_t i0 = chunk * kLsmChunk + j0;
+        if constexpr (kF32) {
+            if (i0 < a.N) {
+                float S4[4], c4[4], v4[4];
+                load4(base + L::kSu * kLsmChunk + j0, S4);
+                if (!init) load4(base + L::kCf * kLsmChunk + j0, c4);
+                load4(base + L::kVu * kLsmChunk + j0, v4);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float iv = lsm_intrinsic<float>(a.right, S4[q], K);
+                    if (init) {
+                        c4[q] = iv;
+                    } else {
+                        const float hold = continuation_f32(cuf, fmaf(S4[q], inv_Kf, -cxuf), v4[q] - cvuf);
+                        c4[q] = (iv > 0.0f && iv > hold) ? iv : c4[q] * disc;
+                    }
+                }
+                store4(cf + i0, c4);  // i0 + 3 < ld: rows are padded to a multiple of 4
+                if (gram) {
+                    float Sg4[4], vg4[4], x[4], w[4], y[4], one[4];
+                    load4(base + L::kSg * kLsmChunk + j0, Sg4);
+                    load4(base + L::kVg * kLsmChunk + j0, vg4);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const bool itm = i0 + q < a.N && lsm_intrinsic<float>(a.right, Sg4[q], K) > 0.0f;
+                        x[q] = itm ? fmaf(Sg4[q], inv_Kf, -cxgf) : 0.0f;
+                        w[q] = itm ? vg4[q] - cvgf : 0.0f;
+                        y[q] = itm ? c4[q] * disc : 0.0f;
+                        one[q] = itm ? 1.0f : 0.0f;
+                    }
+                    accumulate_f32x2(acc2, make_float2(x[0], x[1]), make_float2(w[0], w[1]),
+                                     make_float2(y[0], y[1]), make_float2(one[0], one[1]));
+                    accumulate_f32x2(acc2, make_float2(x[2], x[3]), make_float2(w[2], w[3]),
+                                     make_float2(y[2], y[3]), make_float2(one[2], one[3]));
+                }
+            }
+            if ((k & (kF32Flush - 1)) == kF32Flush - 1) flush();
+            continue;
+        }
         if (i0 < a.N) {
             R S4[4], c4[4], v4[4] = {R(0), R(0), R(0), R(0)};
             load4(base + L::kSu * kLsmChunk + j0, S4);
@@ -573,9 +704,9 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
                 }
             }
         }
-        __syncthreads();  // the stage is refilled by the next iteration's copies
     }
     if (!gram) return;
+    flush();
     // block reduction of the NACC sums
     __shared__ double s_red[kLsmBlock / 32][NACC];
     __shared__ bool s_last;
