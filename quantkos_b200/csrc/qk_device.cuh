@@ -345,34 +345,33 @@ template <>
 __device__ __forceinline__ void step_qe<float>(const StepConst<float> &p, float &S, float &v, float Zv, float Zind) {
     const float m = __fmaf_rn(v, p.exp_mkdt, p.theta_m);
     const float s2 = __fmaf_rn(v, p.s2f1, p.s2f2);
+    const float m2 = __fmul_rn(m, m);
+    // the quadratic regime unconditionally (the common case, no branch before its
+    // SFU chain); the other regimes overwrite its result
     float vn, logM;
+    qe_quadratic_f32(p, m, m2, s2, Zv, vn, logM);
     if (m <= p.eps) {
         vn = 0.0f;
         logM = 0.0f;
-    } else {
-        const float m2 = __fmul_rn(m, m);
-        if (s2 <= __fmul_rn(p.eps, m2)) {
-            vn = m;
-            logM = 0.0f;
-        } else if (s2 <= __fmul_rn(p.psi_c, m2)) {
-            qe_quadratic_f32(p, m, m2, s2, Zv, vn, logM);
+    } else if (s2 <= __fmul_rn(p.eps, m2)) {
+        vn = m;
+        logM = 0.0f;
+    } else if (!(s2 <= __fmul_rn(p.psi_c, m2))) {
+        // exponential branch (rare at the usual parameters): as the generic step
+        const float inv_m = ptx_rcp(m);
+        const float psi = s2 * inv_m * inv_m;
+        const float pz = Math<float>::div(psi - 1.0f, psi + 1.0f);
+        const float beta = (1.0f - pz) * inv_m;
+        const float U = 0.5f * (1.0f + erff(Zv * p.inv_sqrt2));
+        if (U <= pz) {
+            vn = 0.0f;
         } else {
-            // exponential branch (rare at the usual parameters): as the generic step
-            const float inv_m = ptx_rcp(m);
-            const float psi = s2 * inv_m * inv_m;
-            const float pz = Math<float>::div(psi - 1.0f, psi + 1.0f);
-            const float beta = (1.0f - pz) * inv_m;
-            const float U = 0.5f * (1.0f + erff(Zv * p.inv_sqrt2));
-            if (U <= pz) {
-                vn = 0.0f;
-            } else {
-                const float safe_U = fminf(U, 1.0f - p.eps);
-                vn = Math<float>::div(Math<float>::log(Math<float>::div(1.0f - pz, 1.0f - safe_U)), beta);
-            }
-            const float safe_A = fminf(p.A, beta - p.eps);
-            const float M = pz + Math<float>::div(beta * (1.0f - pz), beta - safe_A);
-            logM = Math<float>::log(M);
+            const float safe_U = fminf(U, 1.0f - p.eps);
+            vn = Math<float>::div(Math<float>::log(Math<float>::div(1.0f - pz, 1.0f - safe_U)), beta);
         }
+        const float safe_A = fminf(p.A, beta - p.eps);
+        const float M = pz + Math<float>::div(beta * (1.0f - pz), beta - safe_A);
+        logM = Math<float>::log(M);
     }
     qe_spot_f32(p, S, v, vn, logM, Zind);
     v = vn;
@@ -423,11 +422,9 @@ __device__ __forceinline__ void step_qe_two_f32(const StepConst<float> &p, float
     const float2 em2 = __fmul2_rn(f2(p.eps), m2);
     const float2 pm2 = __fmul2_rn(f2(p.psi_c), m2);
     const bool quad = m.x > p.eps && m.y > p.eps && s2.x > em2.x && s2.y > em2.y && s2.x <= pm2.x && s2.y <= pm2.y;
-    if (!quad) {
-        step_qe<float>(p, S.x, v.x, Zv.x, Zind.x);
-        step_qe<float>(p, S.y, v.y, Zv.y, Zind.y);
-        return;
-    }
+    // the quadratic form for both paths first (no branch before the long SFU chain);
+    // a pair not both in the quadratic regime is redone per path below
+    const float2 S_old = S, v_old = v;
     // qe_quadratic_f32, paired
     const float2 two_ip = __fmul2_rn(__fmul2_rn(f2(2.0f), m2), rcp2(s2));
     const float2 t1 = __fadd2_rn(two_ip, f2(-1.0f));
@@ -447,6 +444,12 @@ __device__ __forceinline__ void step_qe_two_f32(const StepConst<float> &p, float
     const float2 ex = __ffma2_rn(sqrt2(isig), Zind, e12);
     S = __fmul2_rn(S, ex2_2(__fmul2_rn(ex, f2(Math<float>::kLog2e))));
     v = vn;
+    if (!quad) {
+        S = S_old;
+        v = v_old;
+        step_qe<float>(p, S.x, v.x, Zv.x, Zind.x);
+        step_qe<float>(p, S.y, v.y, Zv.y, Zind.y);
+    }
 }
 
 // Milstein for two paths: the spot update (the same as Euler's) paired, the

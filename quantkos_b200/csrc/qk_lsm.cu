@@ -171,16 +171,19 @@ __device__ __forceinline__ void accumulate(double *acc, R S, R v, R K, double in
 // FP32 slab with the 6-term basis: the per-path work (centred point, monomials,
 // continuation) in FP32 on path pairs (sm_100 paired FP32 instructions), without
 // branches — a path out of the money contributes the point (0, 0) with weight 0 —
-// and the 21 sums kept in FP32 for kF32Flush chunk rounds (eight paths per
-// accumulator) before the thread adds them to its FP64 sums.  An FP32 partial over
-// eight paths carries a relative rounding error of order 1e-7 — the size of the FP32
-// slab values' own rounding — and partials round independently, so the FP64 totals
-// over N paths stay accurate to far below the Monte Carlo error; the block and grid
-// reductions and the solve remain FP64.
-constexpr int kF32Flush = 4;
+// and the 21 sums kept in FP32 for kF32Flush chunk rounds (64 paths per thread)
+// before the thread adds them to its FP64 sums.  An FP32 partial over 64 paths
+// carries a relative rounding error of order 1e-6 at most, and partials round
+// independently, so the FP64 totals over N paths stay accurate to far below the
+// Monte Carlo error; the block and grid reductions and the solve remain FP64.
+constexpr int kF32Flush = 16;
 
-__device__ __forceinline__ float continuation_f32(const float *c, float x, float w) {
-    return fmaf(w, fmaf(x, c[5], c[4]), fmaf(x, fmaf(x, fmaf(x, c[3], c[2]), c[1]), c[0]));
+// Continuation value of two paths from the 6-term coefficients c (FP32).
+__device__ __forceinline__ float2 continuation_f32x2(const float *c, float2 x, float2 w) {
+    const float2 px = __ffma2_rn(x, __ffma2_rn(x, __ffma2_rn(x, make_float2(c[3], c[3]), make_float2(c[2], c[2])),
+                                              make_float2(c[1], c[1])),
+                                 make_float2(c[0], c[0]));
+    return __ffma2_rn(w, __ffma2_rn(x, make_float2(c[5], c[5]), make_float2(c[4], c[4])), px);
 }
 
 // Same 21 sums as accumulate<R, QK_LSM_POLY_SV>, in FP32 on two paths; one = path
@@ -547,7 +550,7 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
         if constexpr (kF32) {
 #pragma unroll
             for (int j = 0; j < NACC; ++j) {
-                acc[j] += static_cast<double>(acc2[j].x) + static_cast<double>(acc2[j].y);
+                acc[j] += static_cast<double>(acc2[j].x + acc2[j].y);
                 acc2[j] = make_float2(0.0f, 0.0f);
             }
         }
@@ -640,14 +643,20 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
                 load4(base + L::kSu * kLsmChunk + j0, S4);
                 if (!init) load4(base + L::kCf * kLsmChunk + j0, c4);
                 load4(base + L::kVu * kLsmChunk + j0, v4);
+                if (init) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float iv = lsm_intrinsic<float>(a.right, S4[q], K);
-                    if (init) {
-                        c4[q] = iv;
-                    } else {
-                        const float hold = continuation_f32(cuf, fmaf(S4[q], inv_Kf, -cxuf), v4[q] - cvuf);
-                        c4[q] = (iv > 0.0f && iv > hold) ? iv : c4[q] * disc;
+                    for (int q = 0; q < 4; ++q) c4[q] = lsm_intrinsic<float>(a.right, S4[q], K);
+                } else {
+#pragma unroll
+                    for (int h = 0; h < 4; h += 2) {
+                        const float2 x = __ffma2_rn(make_float2(S4[h], S4[h + 1]), make_float2(inv_Kf, inv_Kf),
+                                                    make_float2(-cxuf, -cxuf));
+                        const float2 w = __fadd2_rn(make_float2(v4[h], v4[h + 1]), make_float2(-cvuf, -cvuf));
+                        const float2 hold = continuation_f32x2(cuf, x, w);
+                        const float iv0 = lsm_intrinsic<float>(a.right, S4[h], K);
+                        const float iv1 = lsm_intrinsic<float>(a.right, S4[h + 1], K);
+                        c4[h] = (iv0 > 0.0f && iv0 > hold.x) ? iv0 : c4[h] * disc;
+                        c4[h + 1] = (iv1 > 0.0f && iv1 > hold.y) ? iv1 : c4[h + 1] * disc;
                     }
                 }
                 store4(cf + i0, c4);  // i0 + 3 < ld: rows are padded to a multiple of 4
