@@ -178,12 +178,11 @@ __device__ __forceinline__ void accumulate(double *acc, R S, R v, R K, double in
 // Monte Carlo error; the block and grid reductions and the solve remain FP64.
 constexpr int kF32Flush = 16;
 
-// Continuation value of two paths from the 6-term coefficients c (FP32).
-__device__ __forceinline__ float2 continuation_f32x2(const float *c, float2 x, float2 w) {
-    const float2 px = __ffma2_rn(x, __ffma2_rn(x, __ffma2_rn(x, make_float2(c[3], c[3]), make_float2(c[2], c[2])),
-                                              make_float2(c[1], c[1])),
-                                 make_float2(c[0], c[0]));
-    return __ffma2_rn(w, __ffma2_rn(x, make_float2(c[5], c[5]), make_float2(c[4], c[4])), px);
+// Continuation value of two paths from the 6-term coefficients c (FP32, each
+// duplicated into a pair).
+__device__ __forceinline__ float2 continuation_f32x2(const float2 *c, float2 x, float2 w) {
+    const float2 px = __ffma2_rn(x, __ffma2_rn(x, __ffma2_rn(x, c[3], c[2]), c[1]), c[0]);
+    return __ffma2_rn(w, __ffma2_rn(x, c[5], c[4]), px);
 }
 
 // Same 21 sums as accumulate<R, QK_LSM_POLY_SV>, in FP32 on two paths; one = path
@@ -626,6 +625,13 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
         if (c < n_chunks) issue(c, s, false, true);
         cp_async_commit();
     }
+    // FP32 6-term kernel: the coefficients in registers, as pairs for the paired FMAs
+    float2 cc[kF32 ? 6 : 1];
+    if constexpr (kF32) {
+        __syncthreads();  // cuf stores visible
+#pragma unroll
+        for (int i = 0; i < 6; ++i) cc[i] = make_float2(cuf[i], cuf[i]);
+    }
     for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {
         cp_async_wait_pending<ST - 2>();  // this thread's copies of `chunk` have landed
         __syncthreads();  // ... and every other thread's; all threads are done with chunk k - 1
@@ -652,7 +658,7 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
                         const float2 x = __ffma2_rn(make_float2(S4[h], S4[h + 1]), make_float2(inv_Kf, inv_Kf),
                                                     make_float2(-cxuf, -cxuf));
                         const float2 w = __fadd2_rn(make_float2(v4[h], v4[h + 1]), make_float2(-cvuf, -cvuf));
-                        const float2 hold = continuation_f32x2(cuf, x, w);
+                        const float2 hold = continuation_f32x2(cc, x, w);
                         const float iv0 = lsm_intrinsic<float>(a.right, S4[h], K);
                         const float iv1 = lsm_intrinsic<float>(a.right, S4[h + 1], K);
                         c4[h] = (iv0 > 0.0f && iv0 > hold.x) ? iv0 : c4[h] * disc;

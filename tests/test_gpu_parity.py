@@ -180,6 +180,25 @@ def test_lsm_fp32_close_to_fp64(qk, handle):
     assert p64["price"] > euro["price"]  # early-exercise premium of the put
 
 
+@pytest.mark.parametrize("right,q,n_paths,dates", [
+    (1, 0.0, 50_003, 20),     # put; paths neither a multiple of 4 nor of the 1024-path chunk
+    (0, 0.08, 80_000, 25),    # call with a dividend yield (early exercise pays)
+    (1, 0.0, 30_001, 0),      # put, every step an exercise date
+])
+def test_lsm_fp32_poly_sv_cases_close_to_fp64(qk, handle, right, q, n_paths, dates):
+    """The FP32 slab with the 6-term basis runs its own sweep arithmetic (FP32 on path
+    pairs, partial sums folded into FP64); same draws priced by the FP64 drop-in."""
+    base = dict(S0=100.0, v0=0.04, q=q, scheme=qk.ANDERSEN_QE, n_steps=100, n_paths=n_paths, seed=11,
+                payoffs=[qk.payoff(qk.AMERICAN, right, 100.0)], lsm_basis=qk.LSM_POLY_SV, lsm_dates=dates)
+    p64 = qk.price_plain(qk.make_contract(precision=qk.FP64, **base), None, handle)["legs"][0]
+    p32 = qk.price_batch([qk.make_contract(precision=qk.FP32, **base)], None, handle)[0]["legs"][0]
+    assert abs(p64["price"] - p32["price"]) < 0.25 * p64["std_error"], (p32, p64)
+    assert p32["std_error"] == pytest.approx(p64["std_error"], rel=0.02)
+    euro = qk.price_plain(qk.make_contract(precision=qk.FP64, **{**base, "payoffs": [qk.payoff(0, right, 100.0)]}),
+                          None, handle)["legs"][0]
+    assert p64["price"] >= euro["price"] - 2.0 * euro["std_error"]  # early exercise adds value
+
+
 @pytest.mark.parametrize("model,scheme", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)])
 def test_prices_vs_closed_form(qk, handle, oracle, model, scheme):
     """European call within 3 SE of the Gil-Pelaez price (HestonTest/BatesTest parameters, 512 steps)."""
