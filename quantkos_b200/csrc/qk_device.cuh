@@ -117,15 +117,38 @@ struct Math<float> {
     static __device__ __forceinline__ float u01(uint32_t w) {
         return __fsub_rn(__uint_as_float(0x3F800000u | (w >> 9)), 0.99999994039535522f);
     }
-    // Box-Muller pair: R = sqrt(-2 ln u1), angle = 2*pi*(u2 - 1/2)
+    static constexpr float kU01Offset = 0.99999994039535522f;  // 1 - 2^-24
+    static constexpr float kTwoPi = 6.28318530717958648f;
+    // Box-Muller pair: R = sqrt(-2 ln u1), angle = 2*pi*(u2 - 1/2); IEEE-rounded
+    // operations in a fixed order (box_muller_two repeats them on pairs)
     static __device__ __forceinline__ void box_muller(uint32_t w1, uint32_t w2, float &z1, float &z2) {
         const float u1 = u01(w1);
         const float u2 = u01(w2);
-        const float rad = ptx_sqrt(-2.0f * kLn2 * ptx_lg2(u1));
+        const float rad = ptx_sqrt(__fmul_rn(-2.0f * kLn2, ptx_lg2(u1)));
         float s, c;
-        __sincosf(6.28318530717958648f * (u2 - 0.5f), &s, &c);
-        z1 = rad * c;
-        z2 = rad * s;
+        __sincosf(__fmul_rn(kTwoPi, __fadd_rn(u2, -0.5f)), &s, &c);
+        z1 = __fmul_rn(rad, c);
+        z2 = __fmul_rn(rad, s);
+    }
+    // Two independent Box-Muller pairs, (a1, a2) and (b1, b2): the same operations as
+    // box_muller with the FP32 multiplies and adds on the paired pipe, so each pair
+    // gets the same bits as from box_muller.  z1 = (z1 of a, z1 of b), z2 likewise.
+    static __device__ __forceinline__ void box_muller_two(uint32_t a1, uint32_t a2, uint32_t b1, uint32_t b2,
+                                                          float2 &z1, float2 &z2) {
+        const float2 off = make_float2(-kU01Offset, -kU01Offset);
+        const float2 u1 = __fadd2_rn(make_float2(__uint_as_float(0x3F800000u | (a1 >> 9)),
+                                                 __uint_as_float(0x3F800000u | (b1 >> 9))), off);
+        const float2 u2 = __fadd2_rn(make_float2(__uint_as_float(0x3F800000u | (a2 >> 9)),
+                                                 __uint_as_float(0x3F800000u | (b2 >> 9))), off);
+        const float2 t = __fmul2_rn(make_float2(-2.0f * kLn2, -2.0f * kLn2),
+                                    make_float2(ptx_lg2(u1.x), ptx_lg2(u1.y)));
+        const float2 rad = make_float2(ptx_sqrt(t.x), ptx_sqrt(t.y));
+        const float2 ang = __fmul2_rn(make_float2(kTwoPi, kTwoPi), __fadd2_rn(u2, make_float2(-0.5f, -0.5f)));
+        float sa, ca, sb, cb;
+        __sincosf(ang.x, &sa, &ca);
+        __sincosf(ang.y, &sb, &cb);
+        z1 = __fmul2_rn(rad, make_float2(ca, cb));
+        z2 = __fmul2_rn(rad, make_float2(sa, sb));
     }
 };
 

@@ -98,44 +98,45 @@ struct RegKeys {
 };
 
 // The step's first Poisson uniform decides whether a jump happened (Knuth's loop
-// continues only if it is >= exp(-lambda dt)).  FP32 compares the word directly:
-// (w >> 9) >= kmin  <=>  u01(w) >= exp(-lambda dt) in float, kmin precomputed exactly.
+// continues only if it is >= exp(-lambda dt)).
+//
+// FP32: the uniform's 23 bits are k = hi:lo.  hi (18 bits) are the low 9 bits of the
+// step's two normal words — FP32 Box-Muller reads only their top 23 bits, so hi is
+// independent of the normals — and lo (5 bits) the top bits of word n mod 4 of block
+// (n/4, path, stream, domain 2).  The test k >= kmin (equivalent to
+// u01 >= exp(-lambda dt) in float, kmin precomputed exactly) cannot pass while
+// hi < kmin >> 5, so the common step compares hi alone and lo is drawn only past that
+// threshold (about lambda dt of the steps).
+__device__ __forceinline__ uint32_t poisson_hi_f32(uint32_t wa, uint32_t wb) {
+    return ((wa & 0x1FFu) << 9) | (wb & 0x1FFu);
+}
+
+// pois: FP32 the 18 high bits (poisson_hi_f32), FP64 the full word.  On a jump,
+// `word` holds the full first-uniform word (top 23 bits k in FP32).
 template <class R>
-__device__ __forceinline__ bool jump_test(uint32_t word, const StepConst<R> &p, uint32_t kmin) {
+__device__ __forceinline__ bool jump_first(uint32_t pois, const StepConst<R> &p, uint32_t kmin, uint32_t k0,
+                                           uint32_t k1, uint32_t path, uint32_t stream, int n, uint32_t &word) {
     if constexpr (sizeof(R) == 4) {
+        if (pois < (kmin >> 5)) return false;
+        const U4 q = philox4x32_10(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u}, k0, k1);
+        const int j = n & 3;
+        const uint32_t w = j == 0 ? q.x : (j == 1 ? q.y : (j == 2 ? q.z : q.w));
+        word = ((pois << 5) | (w >> 27)) << 9;
         return (word >> 9) >= kmin;
     } else {
-        return Math<R>::u01(word) >= p.exp_m_lambda_dt;
+        word = pois;
+        return Math<R>::u01(pois) >= p.exp_m_lambda_dt;
     }
 }
 
-// FP32 first Poisson uniform of step n: 23 bits k = hi:lo.  hi (18 bits) are the low
-// 9 bits of the step's two normal words — FP32 Box-Muller reads only their top 23
-// bits, so hi is independent of the normals — and lo (5 bits) the top bits of word
-// n mod 4 of block (n/4, path, stream, domain 2), drawn only when hi alone cannot
-// decide the jump test (hi >= kmin >> 5: about lambda dt of the steps).  Returns a
-// word whose top 23 bits hold k (what jump_test and u01 read); below the threshold
-// the low part is left zero, which cannot change the (negative) test.
-template <class Gen>
-__device__ __forceinline__ uint32_t poisson_word_f32(uint32_t wa, uint32_t wb, uint32_t kmin, const Gen &gen,
-                                                     uint32_t path, uint32_t stream, int n) {
-    const uint32_t hi = ((wa & 0x1FFu) << 9) | (wb & 0x1FFu);
-    if (hi < (kmin >> 5)) return hi << 14;
-    const U4 q = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
-    const int j = n & 3;
-    const uint32_t w = j == 0 ? q.x : (j == 1 ? q.y : (j == 2 ? q.z : q.w));
-    return ((hi << 5) | (w >> 27)) << 9;
-}
-
-// Words of the first Poisson uniforms of steps n and n+1 (n even) from the normal
-// block w of those steps: FP32 as above; FP64 word n mod 4 of the domain-2 block wp
+// First-Poisson-uniform inputs of steps n and n+1 (n even): FP32 the high bits from
+// the normal block w of those steps; FP64 word n mod 4 of the domain-2 block wp
 // (fetched by the caller every fourth step).
-template <class R, class Gen>
-__device__ __forceinline__ void poisson_words(const U4 &w, const U4 &wp, uint32_t kmin, const Gen &gen,
-                                              uint32_t path, uint32_t stream, int n, uint32_t &p0, uint32_t &p1) {
+template <class R>
+__device__ __forceinline__ void poisson_words(const U4 &w, const U4 &wp, int n, uint32_t &p0, uint32_t &p1) {
     if constexpr (sizeof(R) == 4) {
-        p0 = poisson_word_f32(w.x, w.y, kmin, gen, path, stream, n);
-        p1 = poisson_word_f32(w.z, w.w, kmin, gen, path, stream, n + 1);
+        p0 = poisson_hi_f32(w.x, w.y);
+        p1 = poisson_hi_f32(w.z, w.w);
     } else {
         const bool lo = (n & 3) == 0;
         p0 = lo ? wp.x : wp.z;
@@ -151,8 +152,9 @@ __device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st
     Math<R>::box_muller(wa, wb, z1, z2);
     heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
     if constexpr (MODEL == kBates) {
-        if (jump_test<R>(wpois, p, kmin)) {
-            PhiloxJumpDraws<R> d{k0, k1, path, stream, static_cast<uint32_t>(n), Math<R>::u01(wpois), 1, 0, U4{0, 0, 0, 0}};
+        uint32_t word;
+        if (jump_first<R>(wpois, p, kmin, k0, k1, path, stream, n, word)) {
+            PhiloxJumpDraws<R> d{k0, k1, path, stream, static_cast<uint32_t>(n), Math<R>::u01(word), 1, 0, U4{0, 0, 0, 0}};
             st.S *= jump_factor<R>(p, d.first, d);
         }
     }
@@ -179,7 +181,7 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
                 if constexpr (sizeof(R) == 8) {
                     if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
                 }
-                poisson_words<R>(w, wp, kmin, gen, path, stream, n, pw0, pw1);
+                poisson_words<R>(w, wp, n, pw0, pw1);
             }
             one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
             track(st, blk);
@@ -195,7 +197,7 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
                 if constexpr (sizeof(R) == 8) {
                     if ((n & 3) == 0) wp = gen(U4{static_cast<uint32_t>(n >> 2), path, stream, 2u});
                 }
-                poisson_words<R>(w, wp, kmin, gen, path, stream, n, pw0, pw1);
+                poisson_words<R>(w, wp, n, pw0, pw1);
             }
             one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
             track(st, blk);
@@ -214,33 +216,42 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
                                              uint32_t wa2, uint32_t wb1, uint32_t wb2, uint32_t pois_a,
                                              uint32_t pois_b, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path_a,
                                              uint32_t path_b, uint32_t stream, int n) {
-    R za1, za2, zb1, zb2;
-    Math<R>::box_muller(wa1, wa2, za1, za2);
-    if constexpr (NEG) {
-        zb1 = -za1;
-        zb2 = -za2;
-    } else {
-        Math<R>::box_muller(wb1, wb2, zb1, zb2);
-    }
     if constexpr (sizeof(R) == 4) {
-        // both paths in one paired FP32 step
+        // both paths' normals (paired Box-Muller unless b mirrors a), then one paired step
+        float2 Z1, Z2;
+        if constexpr (NEG) {
+            float za1, za2;
+            Math<float>::box_muller(wa1, wa2, za1, za2);
+            Z1 = make_float2(za1, -za1);
+            Z2 = make_float2(za2, -za2);
+        } else {
+            Math<float>::box_muller_two(wa1, wa2, wb1, wb2, Z1, Z2);
+        }
         float2 S2 = make_float2(a.S, b.S), v2 = make_float2(a.v, b.v);
-        if constexpr (SCHEME == kQE) step_qe_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
-        else if constexpr (SCHEME == kMilstein)
-            step_milstein_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
-        else step_euler_two_f32(p, S2, v2, make_float2(za1, zb1), make_float2(za2, zb2));
+        if constexpr (SCHEME == kQE) step_qe_two_f32(p, S2, v2, Z1, Z2);
+        else if constexpr (SCHEME == kMilstein) step_milstein_two_f32(p, S2, v2, Z1, Z2);
+        else step_euler_two_f32(p, S2, v2, Z1, Z2);
         a.S = S2.x;
         b.S = S2.y;
         a.v = v2.x;
         b.v = v2.y;
     } else {
+        R za1, za2, zb1, zb2;
+        Math<R>::box_muller(wa1, wa2, za1, za2);
+        if constexpr (NEG) {
+            zb1 = -za1;
+            zb2 = -za2;
+        } else {
+            Math<R>::box_muller(wb1, wb2, zb1, zb2);
+        }
         heston_step<R, SCHEME>(p, a.S, a.v, za1, za2);
         heston_step<R, SCHEME>(p, b.S, b.v, zb1, zb2);
     }
     if constexpr (MODEL == kBates) {
+        uint32_t word;
         if constexpr (NEG) {
-            if (jump_test<R>(pois_a, p, kmin)) {
-                PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(pois_a), 1, 0,
+            if (jump_first<R>(pois_a, p, kmin, k0, k1, path_a, stream, n, word)) {
+                PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(word), 1, 0,
                                      U4{0, 0, 0, 0}};
                 R fa, fb;
                 jump_factor_pair<R>(p, d.first, d, fa, fb);
@@ -248,13 +259,13 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
                 b.S *= fb;
             }
         } else {
-            if (jump_test<R>(pois_a, p, kmin)) {
-                PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(pois_a), 1, 0,
+            if (jump_first<R>(pois_a, p, kmin, k0, k1, path_a, stream, n, word)) {
+                PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(word), 1, 0,
                                      U4{0, 0, 0, 0}};
                 a.S *= jump_factor<R>(p, d.first, d);
             }
-            if (jump_test<R>(pois_b, p, kmin)) {
-                PhiloxJumpDraws<R> d{k0, k1, path_b, stream, static_cast<uint32_t>(n), Math<R>::u01(pois_b), 1, 0,
+            if (jump_first<R>(pois_b, p, kmin, k0, k1, path_b, stream, n, word)) {
+                PhiloxJumpDraws<R> d{k0, k1, path_b, stream, static_cast<uint32_t>(n), Math<R>::u01(word), 1, 0,
                                      U4{0, 0, 0, 0}};
                 b.S *= jump_factor<R>(p, d.first, d);
             }
@@ -289,8 +300,8 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
                         if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
                     }
                 }
-                poisson_words<R>(wa, pa, kmin, gen, path_a, stream, n, qa0, qa1);
-                if constexpr (!NEG) poisson_words<R>(wb, pb, kmin, gen, path_b, stream, n, qb0, qb1);
+                poisson_words<R>(wa, pa, n, qa0, qa1);
+                if constexpr (!NEG) poisson_words<R>(wb, pb, n, qb0, qb1);
             }
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
                                                 path_b, stream, n);
@@ -315,8 +326,8 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
                         if constexpr (!NEG) pb = gen(U4{static_cast<uint32_t>(n >> 2), path_b, stream, 2u});
                     }
                 }
-                poisson_words<R>(wa, pa, kmin, gen, path_a, stream, n, qa0, qa1);
-                if constexpr (!NEG) poisson_words<R>(wb, pb, kmin, gen, path_b, stream, n, qb0, qb1);
+                poisson_words<R>(wa, pa, n, qa0, qa1);
+                if constexpr (!NEG) poisson_words<R>(wb, pb, n, qb0, qb1);
             }
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
                                                 path_b, stream, n);
