@@ -300,6 +300,9 @@ def run_other_workload(args) -> None:
                     gpu_launches=tf["launches"])
     else:  # serve
         arrivals, contracts = W.serving_stream(args.requests)
+        # launch shapes per kernel kind from the autotuner on a sample of the stream
+        # (untimed); the server's lanes take them from h
+        tuned = [] if args.no_autotune else h.autotune(contracts[:256], None, reps=1)
         srv = qk.Server(h, 0, 512)
         # warm both lanes
         for c in contracts[:8]:
@@ -357,7 +360,9 @@ def run_other_workload(args) -> None:
                             "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
                             "sample": len(sample), "sample_plain_fp64_contracts_per_s": len(sample) / (t_plain * 1e-3),
                             "sample_batched_contracts_per_s": len(sample) / (t_batch * 1e-3),
-                            "sample_mean_se_ratio_batched_over_plain": se_ratio},
+                            "sample_mean_se_ratio_batched_over_plain": se_ratio,
+                            "autotune": [{k: r[k] for k in ("model", "scheme", "tiles_per_warp", "guided_tail",
+                                                            "paths_per_lane")} for r in tuned]},
                     gpu_launches=None)
     pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     line["clocks"] = sampler.summary(pk.get("sm_max_mhz", 1965.0))

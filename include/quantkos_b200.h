@@ -312,7 +312,9 @@ qk_status qk_run_config(qk_handle *h, const qk_config *c, qk_result *out, double
 /* ---------------------------------------------------------------- serving
  * A continuous-batching request loop.  Requests are admitted by the HBM their
  * LSM slabs and partials need (budget in MiB; 0 = 80% of free HBM), batched with
- * whatever else has arrived, and their results polled by ticket. */
+ * whatever else has arrived, and their results polled by ticket.  The lanes use
+ * h's device and the launch shapes h holds when the server starts (defaults, or
+ * those set by qk_autotune / qk_tune_set). */
 typedef struct qk_server qk_server;
 typedef struct qk_serve_stats {
     int64_t submitted, completed, rejected;

@@ -159,6 +159,33 @@ def test_server_result_alone_equals_in_the_mix(qk, handle):
     assert st["p50_ms"] > 0 and st["p99_ms"] >= st["p50_ms"]
 
 
+def test_server_lanes_take_the_handles_launch_shapes(qk, handle):
+    """qk_serve_start gives its lanes the launch shapes of the handle it starts from: a request
+    served alone equals, bit for bit, qk_price_batch on that handle with the same shapes, while
+    the default shapes merge the moments in other groupings (last-bit differences)."""
+    legs = [qk.payoff(qk.EUROPEAN, qk.CALL, 100.0), qk.payoff(qk.ASIAN, qk.CALL, 100.0),
+            qk.payoff(qk.BARRIER_UP_OUT, qk.CALL, 100.0, 130.0), qk.payoff(qk.LOOKBACK_FLOATING, qk.PUT, 100.0),
+            qk.payoff(qk.BINARY_CASH, qk.CALL, 105.0)]
+    c = qk.make_contract(model=qk.BATES, scheme=qk.ANDERSEN_QE, lambda_j=0.1, mu_j=-0.05, sigma_j=0.1,
+                         n_steps=64, n_paths=300_000, seed=5, precision=qk.FP32, payoffs=legs)
+    key = lambda r: [(g["price"], g["std_error"]) for g in r["legs"]]
+    default = key(qk.price_batch([c], None, handle)[0])
+    handle.tune_set(qk.FP32, qk.BATES, qk.ANDERSEN_QE, 4, True, 2)
+    try:
+        tuned = key(qk.price_batch([c], None, handle)[0])
+        with qk.Server(handle, 0, 4) as srv:
+            t = srv.submit(c)
+            got = None
+            while got is None:
+                got = srv.poll(t, 1000)
+    finally:
+        handle.tune_reset()
+    assert key(got) == tuned
+    assert tuned != default
+    for (p1, s1), (p0, s0) in zip(tuned, default):
+        assert p1 == pytest.approx(p0, rel=1e-12, abs=1e-15) and s1 == pytest.approx(s0, rel=1e-9)
+
+
 def test_server_admission_rejects_oversized(qk, handle):
     from quantkos_b200 import workloads as W
     big = W.american_lsm(n_paths=4_000_000)
