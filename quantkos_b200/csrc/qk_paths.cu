@@ -145,11 +145,9 @@ __device__ __forceinline__ void poisson_words(const U4 &w, const U4 &wp, int n, 
 }
 
 template <class R, int MODEL, int SCHEME>
-__device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st, uint32_t wa, uint32_t wb,
-                                         uint32_t wpois, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path,
-                                         uint32_t stream, int n) {
-    R z1, z2;
-    Math<R>::box_muller(wa, wb, z1, z2);
+__device__ __forceinline__ void one_step_z(const StepConst<R> &p, PathState<R> &st, R z1, R z2, uint32_t wpois,
+                                           uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path, uint32_t stream,
+                                           int n) {
     heston_step<R, SCHEME>(p, st.S, st.v, z1, z2);
     if constexpr (MODEL == kBates) {
         uint32_t word;
@@ -158,6 +156,15 @@ __device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st
             st.S *= jump_factor<R>(p, d.first, d);
         }
     }
+}
+
+template <class R, int MODEL, int SCHEME>
+__device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st, uint32_t wa, uint32_t wb,
+                                         uint32_t wpois, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path,
+                                         uint32_t stream, int n) {
+    R z1, z2;
+    Math<R>::box_muller(wa, wb, z1, z2);
+    one_step_z<R, MODEL, SCHEME>(p, st, z1, z2, wpois, kmin, k0, k1, path, stream, n);
 }
 
 template <class R, int MODEL, int SCHEME, class Gen, class Sink>
@@ -183,10 +190,21 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
                 }
                 poisson_words<R>(w, wp, n, pw0, pw1);
             }
-            one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
-            track(st, blk);
-            sink(n, st.S, st.v);
-            one_step<R, MODEL, SCHEME>(p, st, w.z, w.w, pw1, kmin, k0, k1, path, stream, n + 1);
+            if constexpr (sizeof(R) == 4) {
+                // the normals of both steps (independent of the path state) in one paired
+                // Box-Muller; the same bits as two one-pair calls
+                float2 Z1, Z2;
+                Math<float>::box_muller_two(w.x, w.y, w.z, w.w, Z1, Z2);
+                one_step_z<R, MODEL, SCHEME>(p, st, Z1.x, Z2.x, pw0, kmin, k0, k1, path, stream, n);
+                track(st, blk);
+                sink(n, st.S, st.v);
+                one_step_z<R, MODEL, SCHEME>(p, st, Z1.y, Z2.y, pw1, kmin, k0, k1, path, stream, n + 1);
+            } else {
+                one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
+                track(st, blk);
+                sink(n, st.S, st.v);
+                one_step<R, MODEL, SCHEME>(p, st, w.z, w.w, pw1, kmin, k0, k1, path, stream, n + 1);
+            }
             track(st, blk);
             sink(n + 1, st.S, st.v);
         }
