@@ -468,10 +468,21 @@ __device__ __forceinline__ void step_qe_two_f32(const StepConst<float> &p, float
     S = __fmul2_rn(S, ex2_2(__fmul2_rn(ex, f2(Math<float>::kLog2e))));
     v = vn;
     if (!quad) {
+        // one copy of the one-path step for both paths (rare; keeps the loop body small)
         S = S_old;
         v = v_old;
-        step_qe<float>(p, S.x, v.x, Zv.x, Zind.x);
-        step_qe<float>(p, S.y, v.y, Zv.y, Zind.y);
+#pragma unroll 1
+        for (int i = 0; i < 2; ++i) {
+            float Si = i ? S.y : S.x, vi = i ? v.y : v.x;
+            step_qe<float>(p, Si, vi, i ? Zv.y : Zv.x, i ? Zind.y : Zind.x);
+            if (i) {
+                S.y = Si;
+                v.y = vi;
+            } else {
+                S.x = Si;
+                v.x = vi;
+            }
+        }
     }
 }
 

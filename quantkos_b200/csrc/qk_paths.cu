@@ -276,6 +276,23 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
                 a.S *= fa;
                 b.S *= fb;
             }
+        } else if constexpr (sizeof(R) == 4) {
+            // the one-compare tests of both paths inline; one copy of the rest of the
+            // jump code for both (rare; keeps the loop body small)
+            const uint32_t kmin_hi = kmin >> 5;
+            if (pois_a >= kmin_hi || pois_b >= kmin_hi) {
+#pragma unroll 1
+                for (int i = 0; i < 2; ++i) {
+                    const uint32_t pois = i ? pois_b : pois_a, path = i ? path_b : path_a;
+                    if (jump_first<R>(pois, p, kmin, k0, k1, path, stream, n, word)) {
+                        PhiloxJumpDraws<R> d{k0, k1, path, stream, static_cast<uint32_t>(n), Math<R>::u01(word), 1, 0,
+                                             U4{0, 0, 0, 0}};
+                        const R f = jump_factor<R>(p, d.first, d);
+                        if (i) b.S *= f;
+                        else a.S *= f;
+                    }
+                }
+            }
         } else {
             if (jump_first<R>(pois_a, p, kmin, k0, k1, path_a, stream, n, word)) {
                 PhiloxJumpDraws<R> d{k0, k1, path_a, stream, static_cast<uint32_t>(n), Math<R>::u01(word), 1, 0,
