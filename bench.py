@@ -43,7 +43,7 @@ METRIC = "path-steps/s"
 # at (measured SFU op rate) / 12 path-steps/s; the FP32/integer work (Philox, the
 # QE algebra) fits under that bound on the 128-lane issue.
 SFU_PER_STEP = 12.0
-DRAM_BYTES_PER_PATH_STEP = 8.77e6 / (1_048_576 * 252)
+DRAM_BYTES_PER_PATH_STEP = 2.09e6 / (1_048_576 * 252)
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -479,7 +479,7 @@ def main() -> None:
     kern_ms = statistics.mean(kernel_ms)
     achieved_ps = path_steps / (kern_ms * 1e-3)
     # DRAM bytes of one path-kernel launch: ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-    # on the 1,048,576-path case at the autotuned shape measured 8.77 MB, i.e. 0.0332 B per
+    # on the 1,048,576-path case at the autotuned shape measured 2.09 MB, i.e. 0.0079 B per
     # path-step (tile records plus write-back of the L2-flush buffer), scaled here to the
     # launch's path-steps.  Algorithmic DRAM bytes of the kernel: 0.
     traffic = DRAM_BYTES_PER_PATH_STEP * path_steps
