@@ -373,14 +373,17 @@ def test_antithetic_reduces_error_and_validates(qk, handle, oracle):
                        None, handle)
 
 
-@pytest.mark.parametrize("model,scheme", [(0, 0), (0, 1), (0, 2), (1, 0), (1, 1), (1, 2)])
-def test_lane_modes_simulate_the_same_paths(qk, handle, model, scheme):
-    """A lane carrying two paths (FP32 Euler and QE stepped as pairs on the paired FP32 pipe)
-    and a lane carrying one path simulate bit-identical paths: prices agree to the rounding of
-    the FP64 moment merge, whose grouping of paths differs between the two shapes."""
+@pytest.mark.parametrize("model,scheme,lam", [(0, 0, 0.0), (0, 1, 0.0), (0, 2, 0.0), (1, 0, 0.3), (1, 1, 0.3),
+                                              (1, 2, 0.3), (1, 0, 25.0), (1, 2, 25.0)])
+def test_lane_modes_simulate_the_same_paths(qk, handle, model, scheme, lam):
+    """A lane carrying two paths (FP32 Box-Muller, Euler and QE stepped as pairs on the paired
+    FP32 pipe, rare code shared by the two paths) and a lane carrying one path simulate
+    bit-identical paths: prices agree to the rounding of the FP64 moment merge, whose grouping
+    of paths differs between the two shapes.  lam = 25 sends about a quarter of the steps
+    through the jump code, often for both paths of a lane at once."""
     legs = [qk.payoff(qk.EUROPEAN, qk.CALL, 100.0), qk.payoff(qk.ASIAN, qk.CALL, 100.0),
             qk.payoff(qk.BARRIER_UP_OUT, qk.CALL, 100.0, 130.0), qk.payoff(qk.BINARY_CASH, qk.CALL, 105.0)]
-    c = qk.make_contract(model=model, scheme=scheme, lambda_j=0.3 if model else 0.0, mu_j=-0.05, sigma_j=0.1,
+    c = qk.make_contract(model=model, scheme=scheme, lambda_j=lam, mu_j=-0.05, sigma_j=0.1,
                          sigma=0.5, n_paths=65_537, n_steps=101, seed=5, precision=qk.FP32, payoffs=legs)
     out = []
     try:
