@@ -2,6 +2,7 @@
 // (task list) of one pricing call.
 #pragma once
 
+#include <array>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -64,6 +65,15 @@ constexpr int kLsmLanes = 4;
 
 }  // namespace qk
 
+// Launch shape of each kernel kind, [precision (FP64, FP32)][model][scheme], that a
+// handle starts with: in FP32 the shapes the autotuner picks on the benchmark
+// workloads (48 tiles per warp slot; two paths per lane with a guided tail, except
+// Heston QE, which runs one path per lane); in FP64 24 tiles and one path per lane.
+using ShapeTable = std::array<std::array<std::array<int, 3>, 2>, 2>;
+constexpr ShapeTable kDefaultTilesPerWarp = {{{{{{24, 24, 24}}, {{24, 24, 24}}}}, {{{{48, 48, 48}}, {{48, 48, 48}}}}}};
+constexpr ShapeTable kDefaultGuidedTail = {{{{{{0, 0, 0}}, {{0, 0, 0}}}}, {{{{1, 1, 0}}, {{1, 1, 1}}}}}};
+constexpr ShapeTable kDefaultPathsPerLane = {{{{{{1, 1, 1}}, {{1, 1, 1}}}}, {{{{2, 2, 1}}, {{2, 2, 2}}}}}};
+
 struct qk_handle {
     int device = 0;
     int sm_count = 148;
@@ -80,11 +90,11 @@ struct qk_handle {
     bool prepared = false;
     cudaGraphExec_t graph = nullptr;  // the prepared batch's launch sequence (qk_batch_prepare)
     int64_t graph_launches = 0;
-    // launch shape per kernel kind [precision][model][scheme] (autotuner)
-    // defaults (qk_tune_reset): 24 tiles per warp slot, one path per lane, no guided tail
-    int tune_tpw[2][2][3] = {{{24, 24, 24}, {24, 24, 24}}, {{24, 24, 24}, {24, 24, 24}}};
-    int tune_tail[2][2][3] = {};
-    int tune_lanes[2][2][3] = {{{1, 1, 1}, {1, 1, 1}}, {{1, 1, 1}, {1, 1, 1}}};  // paths per lane: 1 or 2
+    // launch shape per kernel kind [precision][model][scheme] (autotuner); starts at, and
+    // qk_tune_reset restores, the kDefault* tables
+    ShapeTable tune_tpw = kDefaultTilesPerWarp;
+    ShapeTable tune_tail = kDefaultGuidedTail;
+    ShapeTable tune_lanes = kDefaultPathsPerLane;  // paths per lane: 1 or 2
     qk_timing timing{};
     int64_t launches = 0;
     int64_t h2d_bytes = 0, d2h_bytes = 0;

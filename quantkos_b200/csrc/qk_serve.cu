@@ -166,9 +166,9 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
         }
         // the lanes price with the caller's launch shapes (defaults, or those set by
         // qk_autotune / qk_tune_set on h before the start)
-        std::memcpy(lh->tune_tpw, h->tune_tpw, sizeof(h->tune_tpw));
-        std::memcpy(lh->tune_tail, h->tune_tail, sizeof(h->tune_tail));
-        std::memcpy(lh->tune_lanes, h->tune_lanes, sizeof(h->tune_lanes));
+        lh->tune_tpw = h->tune_tpw;
+        lh->tune_tail = h->tune_tail;
+        lh->tune_lanes = h->tune_lanes;
         s->handles.push_back(lh);
     }
     for (qk_handle *lh : s->handles) s->lanes.emplace_back(lane_loop, s, lh);

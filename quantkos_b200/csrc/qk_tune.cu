@@ -28,12 +28,11 @@ namespace {
 constexpr int kTilesPerWarp[] = {4, 8, 12, 24, 48};
 constexpr int kTails[] = {0, 1};
 constexpr int kLanes[] = {1, 2};
-// The handle's default shape of a kind (the initial values in qk_engine.h).
-void default_shape(int precision, int &tpw, int &tail, int &lanes) {
-    (void)precision;
-    tpw = 24;
-    tail = 0;
-    lanes = 1;
+// The handle's default shape of a kind (the tables in qk_engine.h).
+void default_shape(int precision, int model, int scheme, int &tpw, int &tail, int &lanes) {
+    tpw = kDefaultTilesPerWarp[precision][model][scheme];
+    tail = kDefaultGuidedTail[precision][model][scheme];
+    lanes = kDefaultPathsPerLane[precision][model][scheme];
 }
 
 }  // namespace
@@ -43,7 +42,7 @@ extern "C" qk_status qk_tune_reset(qk_handle *h) {
     for (int pr = 0; pr < 2; ++pr)
         for (int md = 0; md < 2; ++md)
             for (int sc = 0; sc < 3; ++sc)
-                default_shape(pr, h->tune_tpw[pr][md][sc], h->tune_tail[pr][md][sc], h->tune_lanes[pr][md][sc]);
+                default_shape(pr, md, sc, h->tune_tpw[pr][md][sc], h->tune_tail[pr][md][sc], h->tune_lanes[pr][md][sc]);
     return QK_OK;
 }
 
@@ -91,7 +90,7 @@ extern "C" qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, 
         std::vector<qk_result> res(sub.size());
         double best = std::numeric_limits<double>::infinity(), dflt = 0.0;
         int dflt_tpw, dflt_tail, dflt_lanes;
-        default_shape(pr, dflt_tpw, dflt_tail, dflt_lanes);
+        default_shape(pr, md, sc, dflt_tpw, dflt_tail, dflt_lanes);
         int best_tpw = dflt_tpw, best_tail = dflt_tail, best_lanes = dflt_lanes;
         for (int lanes : kLanes)
             for (int tpw : kTilesPerWarp)
@@ -104,7 +103,7 @@ extern "C" qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, 
                         const qk_status s = qk::price_contracts(h, sub.data(), static_cast<int32_t>(sub.size()),
                                                                 gsub.data(), res.data(), false);
                         if (s != QK_OK) {
-                            default_shape(pr, h->tune_tpw[pr][md][sc], h->tune_tail[pr][md][sc],
+                            default_shape(pr, md, sc, h->tune_tpw[pr][md][sc], h->tune_tail[pr][md][sc],
                                           h->tune_lanes[pr][md][sc]);
                             return s;
                         }

@@ -170,7 +170,8 @@ def test_server_lanes_take_the_handles_launch_shapes(qk, handle):
                          n_steps=64, n_paths=300_000, seed=5, precision=qk.FP32, payoffs=legs)
     key = lambda r: [(g["price"], g["std_error"]) for g in r["legs"]]
     default = key(qk.price_batch([c], None, handle)[0])
-    handle.tune_set(qk.FP32, qk.BATES, qk.ANDERSEN_QE, 4, True, 2)
+    # one path per lane (the default is two): tiles then group the paths differently
+    handle.tune_set(qk.FP32, qk.BATES, qk.ANDERSEN_QE, 4, False, 1)
     try:
         tuned = key(qk.price_batch([c], None, handle)[0])
         with qk.Server(handle, 0, 4) as srv:
