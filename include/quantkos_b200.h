@@ -202,9 +202,8 @@ qk_status qk_batch_fetch(qk_handle *h, qk_result *out, int32_t n);
  * short "tail" tiles, and whether a lane simulates one path or two independent
  * paths (2u, 2u+1) interleaved.  The reference sizes its path batches from a memory budget
  * (include/core/memory/PathsMCBatchMem.hpp:330-420); there it has no tuner.
- * Defaults: FP32 48 tiles per warp slot, two paths per lane with the guided tail
- * (Heston QE: one path per lane, no guided tail); FP64 24 tiles, one path per lane,
- * no guided tail. */
+ * Defaults: FP32 48 tiles per warp slot, two paths per lane, the guided tail except
+ * for Heston QE; FP64 24 tiles, one path per lane, no guided tail. */
 #define QK_TUNE_KINDS 12
 typedef struct qk_tune_report {
     int32_t n_kinds;                         /* kinds present in the sample */
