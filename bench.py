@@ -64,7 +64,7 @@ def parse_args():
                     help="launch shape 'tiles_per_warp,guided_tail,paths_per_lane' instead of the autotuner")
     ap.add_argument("--paths", type=int, default=N_PATHS,
                     help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
-    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve"], default="bates5",
+    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve", "kinds"], default="bates5",
                     help="bates5 (default): the headline line; the others measure the remaining workloads")
     ap.add_argument("--subset", type=int, default=128, help="batch: contracts priced by both engines")
     ap.add_argument("--requests", type=int, default=20_000, help="serve: number of requests")
@@ -232,6 +232,42 @@ def run_other_workload(args) -> None:
                     config={"workload": "heston_euler_european_call_1048576x252_fp64_plain", "price": r["price"],
                             "std_error": r["std_error"]},
                     gpu_launches=args.steps * h.last_timing()["launches"])
+    elif args.workload == "kinds":
+        # every FP32 kernel kind on one large contract (16.8M x 252, one European leg, the
+        # headline market; Bates jumps as in the headline) at the handle's default shape:
+        # path-kernel time against each kind's SFU bound (Euler and Milstein: Box-Muller
+        # lg2, sqrt, sin, cos + sqrt(v), ex2 = 6 ops per path-step; QE: 12)
+        sfu_ops = h.measure_sfu()
+        kinds, total = [], 0.0
+        with sampler:
+            for model in (qk.HESTON, qk.BATES):
+                for scheme, n_sfu in ((qk.EULER, 6), (qk.IMPLICIT_MILSTEIN, 6), (qk.ANDERSEN_QE, 12)):
+                    c = qk.make_contract(S0=100.0, v0=0.04, r=0.03, q=0.0, model=model, scheme=scheme, kappa=2.0,
+                                         theta=0.04, sigma=0.3, rho=-0.7,
+                                         lambda_j=0.1 if model == qk.BATES else 0.0, mu_j=-0.05, sigma_j=0.10,
+                                         T=1.0, n_steps=N_STEPS, n_paths=N_PATHS, seed=42, precision=qk.FP32,
+                                         payoffs=[qk.payoff(qk.EUROPEAN, qk.CALL, 100.0)])
+                    prep = qk.PreparedBatch([c], None, h)
+                    ms = []
+                    for i in range(max(args.warmup, 3) + args.steps):
+                        flush.fill_(float(i))
+                        torch.cuda.synchronize()
+                        prep.run()
+                        prep.fetch()
+                        if i >= max(args.warmup, 3):
+                            ms.append(h.last_timing()["paths_ms"])
+                    k_ms = statistics.mean(ms)
+                    ps = N_PATHS * N_STEPS / (k_ms * 1e-3)
+                    total += k_ms
+                    kinds.append({"model": "bates" if model == qk.BATES else "heston",
+                                  "scheme": {qk.EULER: "euler", qk.IMPLICIT_MILSTEIN: "milstein",
+                                             qk.ANDERSEN_QE: "qe"}[scheme],
+                                  "kernel_ms": k_ms, "gpath_steps_per_s": ps / 1e9, "sfu_ops_per_step": n_sfu,
+                                  "frac_of_sfu_bound": ps / (sfu_ops / n_sfu)})
+        line.update(value=6 * N_PATHS * N_STEPS / (total * 1e-3), ms_per_step=total / 6, dtype="f32",
+                    config={"workload": f"fp32_kernel_kinds_european_{N_PATHS}x{N_STEPS}", "kinds": kinds,
+                            "sfu_ops_per_s": sfu_ops},
+                    gpu_launches=None)
     elif args.workload == "lsm":
         c32 = W.american_lsm(precision=qk.FP32)
         c64 = W.american_lsm(precision=qk.FP64)
