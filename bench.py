@@ -322,6 +322,28 @@ def run_other_workload(args) -> None:
                                    for a, b in zip(res32, res64) if b["legs"][0]["std_error"] > 0)
         within = sum(abs(a["legs"][0]["price"] - b["legs"][0]["price"]) <= 3.0 * b["legs"][0]["std_error"] + 1e-12
                      for a, b in zip(res32, res64)) / len(sub)
+        # Greeks of the batched FP32 engine against the FP64 drop-in on the same draws (common
+        # random numbers): the difference is precision, not sampling.  Reported relative and in
+        # units of a conservative standard-error bound of each finite difference (sd(X - Y) <=
+        # sd(X) + sd(Y), every bumped price taken with the base price's standard error).
+        def se_bound(c, se, f):
+            hs = c.S0 * g.bump_S_rel
+            hv = c.v0 * g.bump_vol if g.vega_mode == 1 else g.bump_vol
+            return {"delta": se / hs, "gamma": 4 * se / hs ** 2, "vega": se / hv, "vomma": 4 * se / hv ** 2,
+                    "vanna": se / (hs * hv), "rho": se / g.bump_r_abs, "theta": 2 * se / g.bump_T_abs}[f]
+
+        greek_err = {}
+        for f in ("delta", "gamma", "vega", "vomma", "vanna", "rho", "theta"):
+            rel, in_se = [], []
+            for c, a, b in zip(sub64, res32, res64):
+                la, lb = a["legs"][0], b["legs"][0]
+                d = abs(la[f] - lb[f])
+                rel.append(d / max(abs(lb[f]), 1e-12))
+                bound = se_bound(c, lb["std_error"], f)
+                if bound > 0:
+                    in_se.append(d / bound)
+            greek_err[f] = {"median_rel": statistics.median(rel), "median_in_se_bound": statistics.median(in_se),
+                            "max_in_se_bound": max(in_se)}
         line.update(metric="contracts/s", unit="contracts/s", value=len(full) / (ms * 1e-3), ms_per_step=ms,
                     dtype="f32",
                     config={"workload": "mixed_4096_contracts_all_greeks_seed123",
@@ -331,6 +353,7 @@ def run_other_workload(args) -> None:
                             "speedup_vs_plain_fp64_same_subset": t_plain / t_sub,
                             "mean_se_ratio_batched_over_plain": se_ratio,
                             "subset_prices_within_3se_of_fp64": within,
+                            "greeks_fp32_minus_fp64": greek_err,
                             "autotune": [{k: r[k] for k in ("model", "scheme", "tiles_per_warp", "guided_tail",
                                                             "paths_per_lane")} for r in tuned]},
                     gpu_launches=tf["launches"])
