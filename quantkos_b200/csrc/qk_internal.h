@@ -80,7 +80,7 @@ struct TaskDev {
     int64_t tile_begin;    // first queue slot of the task (tiles of a task are consecutive)
     int64_t partial_base;  // first per-tile moments record of the task
     int32_t n_tiles;
-    int32_t ppt;           // rounds of a big tile: a round is one path per lane of a warp
+    int32_t ppt;           // rounds of a big tile: a round is one lane unit (lane_mode) per lane of a warp
     int32_t n_big;         // tiles 0 .. n_big-1 have ppt rounds; the rest (the tail) ppt_tail rounds
     int32_t ppt_tail;
     int64_t chunk_base;    // first merge chunk of the task (two-level merge of the tile records)
