@@ -32,7 +32,7 @@ REFERENCE_ROOT = Path(os.environ.get("QK_REFERENCE_ROOT", "/root/reference"))
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
 SOURCES = ["qk_paths.cu", "qk_lsm.cu", "qk_api.cu", "qk_serve.cu", "qk_config.cu", "qk_tune.cu", "qk_noalloc.cu"]
 
@@ -67,7 +67,7 @@ def build_engine(force: bool = False) -> Path:
         _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"])
     cli_src = CSRC / "qk_cli.cpp"
     if cli_src.exists() and (force or _stale(CLI, [cli_src, LIB])):
-        _run(["g++", "-std=c++17", "-O2", "-o", str(CLI), str(cli_src), f"-I{ROOT / 'include'}",
+        _run(["g++", "-std=c++20", "-O2", "-o", str(CLI), str(cli_src), f"-I{ROOT / 'include'}",
               f"-L{PKG}", "-lquantkos_b200", f"-Wl,-rpath,$ORIGIN"])
     return LIB
 
