@@ -195,6 +195,14 @@ std::vector<int> roles_for(const qk_greeks *g, double T) {
     return roles;
 }
 
+// Asian, barrier and lookback legs read the running sum, max or min of the path;
+// European, binary and American legs only its final spot.
+static bool needs_path_state(const qk_contract &c) {
+    for (int k = 0; k < c.n_payoffs; ++k)
+        if (c.payoffs[k].type >= QK_ASIAN && c.payoffs[k].type <= QK_LOOKBACK_FIXED) return true;
+    return false;
+}
+
 TaskDev make_task(const qk_contract &b, int ppt, int lane_mode) {
     TaskDev t;
     std::memset(&t, 0, sizeof(t));
@@ -218,6 +226,7 @@ TaskDev make_task(const qk_contract &b, int ppt, int lane_mode) {
     const double kd = std::ceil(static_cast<double>(Lf) * 8388608.0 - 0.5);
     t.jump_kmin = static_cast<uint32_t>(std::min(std::max(kd, 0.0), 8388608.0));
     t.lane_mode = b.antithetic ? kLanePair : lane_mode;
+    t.track = needs_path_state(b) ? 1 : 0;
     const int64_t units = lane_units(b.n_paths, t.lane_mode);
     const int64_t tile_units = static_cast<int64_t>(kWarpTilePaths) * ppt;
     t.n_tiles = static_cast<int32_t>((units + tile_units - 1) / tile_units);
@@ -326,7 +335,7 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
     plan.status.assign(n, QK_OK);
     plan.task_of.assign(static_cast<size_t>(n) * kNumRoles, -1);
     // paths per kernel kind (precision, model, scheme): each kind is one launch
-    int64_t kind_paths[2][2][3][3] = {};  // [precision][model][scheme][lane mode]: lane units per launch
+    int64_t kind_paths[2][2][3][3][2] = {};  // [precision][model][scheme][lane mode][track]: lane units per launch
     auto lane_mode_of = [&](const qk_contract &c, int pr) {
         if (c.antithetic) return static_cast<int>(kLanePair);
         if (plain) return static_cast<int>(kLaneOne);
@@ -344,7 +353,7 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         }
         const int pr = plain ? QK_FP64 : cs[i].precision;
         const int lm = lane_mode_of(cs[i], pr);
-        kind_paths[pr][cs[i].model][cs[i].scheme][lm] +=
+        kind_paths[pr][cs[i].model][cs[i].scheme][lm][needs_path_state(cs[i])] +=
             lane_units(cs[i].n_paths, lm) * static_cast<int64_t>(roles_for(g, cs[i].T).size());
     }
     struct Item {
@@ -358,12 +367,13 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         const int pr = plain ? QK_FP64 : cs[i].precision;
         const int lm = lane_mode_of(cs[i], pr);
         const int64_t units = lane_units(cs[i].n_paths, lm);
-        const int64_t launch_units = plain ? units : kind_paths[pr][cs[i].model][cs[i].scheme][lm];
+        const bool trk = needs_path_state(cs[i]);
+        const int64_t launch_units = plain ? units : kind_paths[pr][cs[i].model][cs[i].scheme][lm][trk];
         const int ppt = choose_ppt(units, launch_units, h->sm_count,
                                    plain ? kPlainTilesPerWarp : h->tune_tpw[pr][cs[i].model][cs[i].scheme]);
         const bool tail = !plain && h->tune_tail[pr][cs[i].model][cs[i].scheme];
         const int64_t warp_slots = static_cast<int64_t>(h->sm_count) *
-                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, lm) *
+                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, lm, trk) *
                                    (kPathBlock / 32);
         const qk_greeks *g = plan.g_of(i);
         for (int role : roles_for(g, cs[i].T)) {
@@ -375,10 +385,12 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         }
     }
     if (!plain) {
-        // group by kernel (precision, model, scheme); longest tiles first inside a group
+        // group by kernel (precision, lane mode, path state, model, scheme); longest tiles
+        // first inside a group
         std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
             if (a.t.precision != b.t.precision) return a.t.precision < b.t.precision;
             if (a.t.lane_mode != b.t.lane_mode) return a.t.lane_mode < b.t.lane_mode;
+            if (a.t.track != b.t.track) return a.t.track > b.t.track;
             if (a.t.model != b.t.model) return a.t.model < b.t.model;
             if (a.t.scheme != b.t.scheme) return a.t.scheme < b.t.scheme;
             return a.cost > b.cost;
@@ -447,13 +459,13 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
     if (plan.plain) {
         for (size_t i = 0; i < nt; ++i) {
             const TaskDev &t = plan.tasks[i];
-            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme, t.lane_mode);
+            const int per_sm = price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme, t.lane_mode, t.track);
             const int grid = static_cast<int>(std::min<int64_t>(t.n_tiles, static_cast<int64_t>(h->sm_count) * per_sm));
             // one task: its own queue cursor, its own tile range (prefix of one task = itself)
             const uint64_t seed = static_cast<uint64_t>(t.key0) | (static_cast<uint64_t>(t.key1) << 32);
             QK_CUDA_TRY(launch_price_tiles(t.precision, t.model, t.scheme, grid, h->stream, dt + i, dp + i, 1,
                                            t.tile_begin, t.tile_begin + t.n_tiles, dc + i, dpart, true, seed,
-                                           t.lane_mode));
+                                           t.lane_mode, t.track));
             h->launches++;
         }
     } else {
@@ -462,11 +474,12 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             size_t e = b;
             const TaskDev &tb = plan.tasks[b];
             while (e < nt && plan.tasks[e].precision == tb.precision && plan.tasks[e].model == tb.model &&
-                   plan.tasks[e].scheme == tb.scheme && plan.tasks[e].lane_mode == tb.lane_mode)
+                   plan.tasks[e].scheme == tb.scheme && plan.tasks[e].lane_mode == tb.lane_mode &&
+                   plan.tasks[e].track == tb.track)
                 ++e;
             const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
             const int64_t slots = slots_end - tb.tile_begin;
-            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.lane_mode);
+            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.lane_mode, tb.track);
             const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
             bool uniform_key = true;
             for (size_t i = b; i < e; ++i)
@@ -474,7 +487,7 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
             QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
                                            static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
-                                           uniform_key, seed, tb.lane_mode));
+                                           uniform_key, seed, tb.lane_mode, tb.track));
             h->launches++;
             b = e;
         }

@@ -86,6 +86,7 @@ struct TaskDev {
     int64_t chunk_base;    // first merge chunk of the task (two-level merge of the tile records)
     int32_t n_chunks;      // merge chunks of the task: ceil(n_tiles / kMergeChunkTiles)
     int32_t lane_mode;     // kLaneOne / kLanePair / kLaneTwo: what a lane simulates; tiles count lane units
+    int32_t track;         // 1 if a leg reads the path state (Asian sum, running max / min)
     PayoffSpec pay[QK_MAX_PAYOFFS];
 };
 

@@ -17,10 +17,12 @@ constexpr int kPathMinBlocksFp32 = QK_PATH_MIN_BLOCKS_FP32;  // resident blocks 
 // uniform_key: every task of the launch has Philox key `seed` (round keys go in the
 // kernel parameters); otherwise each task's key is read from its descriptor.
 // lane_mode: what a lane simulates for every task of the launch (TaskDev::lane_mode).
+// track: some task of the launch has a leg that reads the path state (TaskDev::track);
+// false selects the kernel that keeps none.
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
                                unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
-                               int lane_mode = kLaneOne);
+                               int lane_mode = kLaneOne, bool track = true);
 // max_tiles: the largest n_tiles among the tasks (sets the block width).
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
                                TaskMoments *out, int64_t max_tiles = 0);
@@ -38,7 +40,8 @@ cudaError_t launch_slab_paths(int precision, int model, int scheme, uint64_t see
 cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task, const double *z, const double *u,
                               int umax, int n, double *S_out, double *v_out, int *status);
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode = kLaneOne);
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode = kLaneOne,
+                                  bool track = true);
 // Times a kernel of independent ex2.approx chains; returns its duration and MUFU op count.
 cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
                              double *ops);

@@ -167,7 +167,9 @@ __device__ __forceinline__ void one_step(const StepConst<R> &p, PathState<R> &st
     one_step_z<R, MODEL, SCHEME>(p, st, z1, z2, wpois, kmin, k0, k1, path, stream, n);
 }
 
-template <class R, int MODEL, int SCHEME, class Gen, class Sink>
+// TRK: keep the path state that Asian, barrier and lookback legs read (running sum,
+// max, min); false for launches whose legs read only the final spot.
+template <class R, int MODEL, int SCHEME, bool TRK = true, class Gen, class Sink>
 __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
                                               uint32_t k0, uint32_t k1, uint32_t path, uint32_t stream, uint32_t kmin,
                                               PathState<R> &st, Sink &&sink) {
@@ -196,16 +198,16 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
                 float2 Z1, Z2;
                 Math<float>::box_muller_two(w.x, w.y, w.z, w.w, Z1, Z2);
                 one_step_z<R, MODEL, SCHEME>(p, st, Z1.x, Z2.x, pw0, kmin, k0, k1, path, stream, n);
-                track(st, blk);
+                if constexpr (TRK) track(st, blk);
                 sink(n, st.S, st.v);
                 one_step_z<R, MODEL, SCHEME>(p, st, Z1.y, Z2.y, pw1, kmin, k0, k1, path, stream, n + 1);
             } else {
                 one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
-                track(st, blk);
+                if constexpr (TRK) track(st, blk);
                 sink(n, st.S, st.v);
                 one_step<R, MODEL, SCHEME>(p, st, w.z, w.w, pw1, kmin, k0, k1, path, stream, n + 1);
             }
-            track(st, blk);
+            if constexpr (TRK) track(st, blk);
             sink(n + 1, st.S, st.v);
         }
         if (n < n1) {
@@ -218,10 +220,10 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
                 poisson_words<R>(w, wp, n, pw0, pw1);
             }
             one_step<R, MODEL, SCHEME>(p, st, w.x, w.y, pw0, kmin, k0, k1, path, stream, n);
-            track(st, blk);
+            if constexpr (TRK) track(st, blk);
             sink(n, st.S, st.v);
         }
-        st.ssum += static_cast<double>(blk);
+        if constexpr (TRK) st.ssum += static_cast<double>(blk);
     }
 }
 
@@ -308,7 +310,7 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
     }
 }
 
-template <class R, int MODEL, int SCHEME, bool NEG, class Gen, class Sink2>
+template <class R, int MODEL, int SCHEME, bool NEG, bool TRK = true, class Gen, class Sink2>
 __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
                                              uint32_t k0, uint32_t k1, uint32_t path_a, uint32_t path_b,
                                              uint32_t stream, uint32_t kmin, PathState<R> &a, PathState<R> &b,
@@ -340,13 +342,13 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
             }
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
                                                 path_b, stream, n);
-            track(a, blk_a);
-            track(b, blk_b);
+            if constexpr (TRK) track(a, blk_a);
+            if constexpr (TRK) track(b, blk_b);
             sink(n, a.S, a.v, b.S, b.v);
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.z, wa.w, wb.z, wb.w, qa1, qb1, kmin, k0, k1, path_a,
                                                 path_b, stream, n + 1);
-            track(a, blk_a);
-            track(b, blk_b);
+            if constexpr (TRK) track(a, blk_a);
+            if constexpr (TRK) track(b, blk_b);
             sink(n + 1, a.S, a.v, b.S, b.v);
         }
         if (n < n1) {
@@ -366,12 +368,14 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
             }
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
                                                 path_b, stream, n);
-            track(a, blk_a);
-            track(b, blk_b);
+            if constexpr (TRK) track(a, blk_a);
+            if constexpr (TRK) track(b, blk_b);
             sink(n, a.S, a.v, b.S, b.v);
         }
-        a.ssum += static_cast<double>(blk_a);
-        b.ssum += static_cast<double>(blk_b);
+        if constexpr (TRK) {
+            a.ssum += static_cast<double>(blk_a);
+            b.ssum += static_cast<double>(blk_b);
+        }
     }
 }
 
@@ -420,7 +424,7 @@ __device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int
 
 // LANE: kLaneOne (a lane simulates one path), kLanePair (an antithetic pair),
 // kLaneTwo (two independent paths 2u and 2u+1).
-template <class R, int MODEL, int SCHEME, bool UK, int LANE>
+template <class R, int MODEL, int SCHEME, bool UK, int LANE, bool TRK>
 __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp32 : 1)
     price_tiles_kernel(const TaskDev *__restrict__ tasks, const int64_t *__restrict__ prefix, int32_t n_tasks,
                        int64_t slot_begin, int64_t slot_end, unsigned long long *__restrict__ cursor,
@@ -474,10 +478,10 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
                 PathState<R> sa, sb;
                 if (active) {
                     if constexpr (UK) {
-                        simulate_two<R, MODEL, SCHEME, NEG>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1, pa, pb, stream,
+                        simulate_two<R, MODEL, SCHEME, NEG, TRK>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1, pa, pb, stream,
                                                             kmin, sa, sb, NoSink2{});
                     } else {
-                        simulate_two<R, MODEL, SCHEME, NEG>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1, pa, pb,
+                        simulate_two<R, MODEL, SCHEME, NEG, TRK>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1, pa, pb,
                                                             stream, kmin, sa, sb, NoSink2{});
                     }
                 } else {
@@ -502,10 +506,10 @@ __global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp3
                 PathState<R> st;
                 if (active) {
                     if constexpr (UK) {
-                        simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
+                        simulate_path<R, MODEL, SCHEME, TRK>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1,
                                                         static_cast<uint32_t>(unit), stream, kmin, st, NoSink{});
                     } else {
-                        simulate_path<R, MODEL, SCHEME>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
+                        simulate_path<R, MODEL, SCHEME, TRK>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1,
                                                         static_cast<uint32_t>(unit), stream, kmin, st, NoSink{});
                     }
                 } else {
@@ -530,30 +534,34 @@ template <class R>
 using PriceKernel = void (*)(const TaskDev *, const int64_t *, int32_t, int64_t, int64_t, unsigned long long *,
                              Moments *, const PhiloxRoundKeys);
 
-template <class R, bool UK, int LANE>
+template <class R, bool UK, int LANE, bool TRK>
 __host__ PriceKernel<R> price_kernel_for_keys(int model, int scheme) {
     switch (model * 3 + scheme) {
-        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK, LANE>;
-        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK, LANE>;
-        case 2: return price_tiles_kernel<R, kHeston, kQE, UK, LANE>;
-        case 3: return price_tiles_kernel<R, kBates, kEuler, UK, LANE>;
-        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK, LANE>;
-        default: return price_tiles_kernel<R, kBates, kQE, UK, LANE>;
+        case 0: return price_tiles_kernel<R, kHeston, kEuler, UK, LANE, TRK>;
+        case 1: return price_tiles_kernel<R, kHeston, kMilstein, UK, LANE, TRK>;
+        case 2: return price_tiles_kernel<R, kHeston, kQE, UK, LANE, TRK>;
+        case 3: return price_tiles_kernel<R, kBates, kEuler, UK, LANE, TRK>;
+        case 4: return price_tiles_kernel<R, kBates, kMilstein, UK, LANE, TRK>;
+        default: return price_tiles_kernel<R, kBates, kQE, UK, LANE, TRK>;
     }
 }
 
 template <class R, int LANE>
-__host__ PriceKernel<R> price_kernel_for_lane(int model, int scheme, bool uniform_key) {
-    return uniform_key ? price_kernel_for_keys<R, true, LANE>(model, scheme)
-                       : price_kernel_for_keys<R, false, LANE>(model, scheme);
+__host__ PriceKernel<R> price_kernel_for_lane(int model, int scheme, bool uniform_key, bool track) {
+    if (track)
+        return uniform_key ? price_kernel_for_keys<R, true, LANE, true>(model, scheme)
+                           : price_kernel_for_keys<R, false, LANE, true>(model, scheme);
+    return uniform_key ? price_kernel_for_keys<R, true, LANE, false>(model, scheme)
+                       : price_kernel_for_keys<R, false, LANE, false>(model, scheme);
 }
 
 template <class R>
-__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true, int lane_mode = kLaneOne) {
+__host__ PriceKernel<R> price_kernel_for(int model, int scheme, bool uniform_key = true, int lane_mode = kLaneOne,
+                                         bool track = true) {
     switch (lane_mode) {
-        case kLanePair: return price_kernel_for_lane<R, kLanePair>(model, scheme, uniform_key);
-        case kLaneTwo: return price_kernel_for_lane<R, kLaneTwo>(model, scheme, uniform_key);
-        default: return price_kernel_for_lane<R, kLaneOne>(model, scheme, uniform_key);
+        case kLanePair: return price_kernel_for_lane<R, kLanePair>(model, scheme, uniform_key, track);
+        case kLaneTwo: return price_kernel_for_lane<R, kLaneTwo>(model, scheme, uniform_key, track);
+        default: return price_kernel_for_lane<R, kLaneOne>(model, scheme, uniform_key, track);
     }
 }
 
@@ -782,14 +790,14 @@ __global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
                                unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
-                               int lane_mode) {
+                               int lane_mode, bool track) {
     const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
                                                  static_cast<uint32_t>(seed >> 32));
     if (precision == QK_FP32)
-        price_kernel_for<float>(model, scheme, uniform_key, lane_mode)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<float>(model, scheme, uniform_key, lane_mode, track)<<<grid, kPathBlock, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     else
-        price_kernel_for<double>(model, scheme, uniform_key, lane_mode)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<double>(model, scheme, uniform_key, lane_mode, track)<<<grid, kPathBlock, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     return cudaGetLastError();
 }
@@ -885,14 +893,14 @@ cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEven
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode) {
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode, bool track) {
     int nb = 0;
     if (precision == QK_FP32)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<float>(model, scheme, true, lane_mode),
-                                                      kPathBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &nb, price_kernel_for<float>(model, scheme, true, lane_mode, track), kPathBlock, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, price_kernel_for<double>(model, scheme, true, lane_mode),
-                                                      kPathBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &nb, price_kernel_for<double>(model, scheme, true, lane_mode, track), kPathBlock, 0);
     return nb > 0 ? nb : 1;
 }
 
