@@ -867,7 +867,11 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmAr
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_sweep_kernel<R, BASIS>, kLsmBlock, smem);
     if (e != cudaSuccess) return e;
-    const int sgrid = sm_count * std::min(std::max(per_sm, 1), 4);
+    // and no more blocks than chunks: a small job's empty blocks would still launch,
+    // check in on the counter and have their (zero) sums folded by the last block
+    const int64_t n_chunks = (a.ld + kLsmChunk - 1) / kLsmChunk;
+    const int sgrid = static_cast<int>(
+        std::min<int64_t>(static_cast<int64_t>(sm_count) * std::min(std::max(per_sm, 1), 4), std::max<int64_t>(n_chunks, 1)));
     e = cudaMemsetAsync(done, 0, sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
     lsm_sweep_kernel<R, BASIS><<<sgrid, kLsmBlock, smem, s>>>(a, S, V, cf, D - 1, 1, D - 2, coeffs, centre,
