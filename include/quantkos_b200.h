@@ -6,8 +6,7 @@
  * reference project).  This header is the drop-in boundary that replaces them:
  * plain C types, caller-owned host arrays, handle-owned device memory, integer
  * status codes (never abort, never trap).  The C++ wrappers with the
- * reference's own names live in quantkos_b200.hpp; INTEGRATION.md shows the
- * bindings a maintainer adds.
+ * reference's own names live in quantkos_b200.hpp.
  *
  * Threading: a handle is used by one host thread at a time, except
  * qk_serve_submit / qk_serve_poll / qk_serve_cancel, which are thread-safe.
@@ -236,13 +235,19 @@ qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t sc
  * pricing path (a host application owning all GPU memory through its own pool,
  * or a latency-critical caller that cannot take cudaMalloc/cudaFree and their
  * device synchronisation between requests).  Same kernels as qk_price_batch; all
- * scratch lives in one fixed device array of about 4.1 MiB reserved per device
- * when the library loads; nothing is allocated and no handle is needed.
- * Limit: ceil(n_paths / 2048) * n_payoffs <= 131072 (QK_ERR_CAPACITY beyond).
- * The first call on a device looks up the array's address with that device
- * current: make it before any stream capture.  Calls share the array: calls
- * whose GPU work overlaps race, so serialize them.  `stream` is a cudaStream_t
- * (NULL = default stream); the call returns after its work has finished. */
+ * scratch lives in one fixed device array of about 4.1 MiB per device; no handle
+ * is needed.  Limit: ceil(n_paths / 2048) * n_payoffs <= 131072 (QK_ERR_CAPACITY
+ * beyond).  The first call on each device is its set-up and does take device
+ * memory: with that device current it looks up the array's address, and the CUDA
+ * runtime, which loads device code lazily, then reserves the array and loads the
+ * kernels' code on that device.  Make that first call during set-up, before a
+ * memory pool takes the device's free memory, and before any stream capture.
+ * Later calls allocate nothing, except that the first launch of a kernel kind
+ * (precision x model x scheme, with or without path-dependent legs) can make the
+ * driver grow its local-memory reservation: price one small contract of each
+ * kind you will use during set-up.  Calls share the array: calls whose GPU work
+ * overlaps race, so serialize them.  `stream` is a cudaStream_t (NULL = default
+ * stream); the call returns after its work has finished. */
 qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_result *out);
 
 /* ---------------------------------------------------------------- parity harness

@@ -28,6 +28,9 @@ CLI = PKG / "quantkos"
 ORACLE_DIR = ROOT / "oracle"
 ORACLE_LIB = ORACLE_DIR / "libqkoracle.so"
 REF_DIR = ORACLE_DIR / "ref_harness"
+# Where the reference checkout lies: QK_REFERENCE_ROOT, else the build machine's checkout.
+# This build recipe is the only place that names that location; the harness Makefile and
+# the golden-fixture generator take it from here.
 REFERENCE_ROOT = Path(os.environ.get("QK_REFERENCE_ROOT", "/root/reference"))
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")

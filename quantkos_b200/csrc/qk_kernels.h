@@ -42,6 +42,10 @@ cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task
 cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out);
 int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode = kLaneOne,
                                   bool track = true);
+// Loads the device code of every one-path-per-lane pricing kernel (both precisions,
+// every model and scheme, with and without path state) and of the one-block-per-task
+// merge, without launching anything.
+cudaError_t preload_noalloc_kernels();
 // Times a kernel of independent ex2.approx chains; returns its duration and MUFU op count.
 cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
                              double *ops);

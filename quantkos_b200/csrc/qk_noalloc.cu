@@ -7,18 +7,27 @@
 // acceptable between requests.  qk_price_noalloc serves them: it runs the same
 // fused path kernel and tile merge as qk_price_batch, but every byte of scratch
 // it needs (task descriptor, queue cursor, per-tile moment records, merged
-// moments) lives in one file-scope device array of fixed size, reserved when
-// the library is loaded.  No handle is involved and nothing is allocated.
+// moments) lives in one file-scope device array of fixed size.  No handle is
+// involved, and after the first call on a device nothing is allocated.
 //
 // Limits and rules of use:
-//   * scratch is kNoAllocScratchBytes (about 4.1 MiB) per device that loads the
-//     library, held until the process exits;
+//   * scratch is kNoAllocScratchBytes (about 4.1 MiB) per device, held until the
+//     process exits;
+//   * the first call on each device is its set-up, and that call does take device
+//     memory: the CUDA runtime loads device code lazily, so the array is reserved
+//     and the pricing kernels' code is loaded on that device then (the set-up
+//     loads every kernel kind the entry point can launch).  Make the first call
+//     during the caller's own set-up, before its memory pool takes the device's
+//     free memory.  The first launch of a kernel kind can also make the driver
+//     grow its per-thread local-memory reservation, so a caller that must see no
+//     allocation at all afterwards prices one small contract of each kind
+//     (precision x model x scheme, with or without path-dependent legs) it will
+//     use during set-up;
 //   * one forward contract (no American leg), no Greeks, at most
 //     kNoAllocMaxRecords tile records: ceil(n_paths / 2048) * n_payoffs <= 131072
 //     (for example 33,554,432 paths with 8 legs, 53,687,091 with 5);
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call before
-//     any stream capture;
+//   * the set-up looks up the array's device address (cudaGetSymbolAddress) with
+//     that device current; make the first call before any stream capture;
 //   * every call shares the one array and it keeps the previous call's contents;
 //     the queue cursor is cleared at the start of each call, every other field is
 //     overwritten before it is read.  Calls whose GPU work overlaps (different
@@ -67,6 +76,13 @@ qk_status scratch_for_current_device(void **out) {
         if (e != cudaSuccess || !p)
             return qk::fail(QK_ERR_CUDA, std::string("qk_price_noalloc: cudaGetSymbolAddress failed: ") +
                                              cudaGetErrorString(e));
+        // load the device code of every kernel this entry point launches now, so that
+        // later calls do not load it (with lazy module loading, a kernel's code is
+        // loaded into device memory on its first use)
+        e = qk::preload_noalloc_kernels();
+        if (e != cudaSuccess)
+            return qk::fail(QK_ERR_CUDA, std::string("qk_price_noalloc: loading the kernels failed: ") +
+                                             cudaGetErrorString(e));
         g_scratch_ptr[dev] = p;
     }
     *out = g_scratch_ptr[dev];
@@ -109,7 +125,7 @@ extern "C" qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_res
     cudaGetDevice(&dev);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int per_sm = qk::price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme);
+    const int per_sm = qk::price_tiles_max_blocks_per_sm(t.precision, t.model, t.scheme, t.lane_mode, t.track != 0);
     const int grid = static_cast<int>(std::min<int64_t>((t.n_tiles + 7) / 8, static_cast<int64_t>(sms) * per_sm));
     qk::Moments m[QK_MAX_PAYOFFS];
     cudaError_t e = cudaMemcpyAsync(d_task, &t, sizeof(t), cudaMemcpyHostToDevice, st);
@@ -117,7 +133,7 @@ extern "C" qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_res
     if (e == cudaSuccess) e = cudaMemsetAsync(d_cursor, 0, sizeof(unsigned long long), st);  // queue starts empty
     if (e == cudaSuccess)
         e = qk::launch_price_tiles(t.precision, t.model, t.scheme, std::max(grid, 1), st, d_task, d_prefix, 1, 0,
-                                   t.n_tiles, d_cursor, d_partials, true, c->seed);
+                                   t.n_tiles, d_cursor, d_partials, true, c->seed, t.lane_mode, t.track != 0);
     if (e == cudaSuccess) e = qk::launch_merge_tasks(1, st, d_task, d_partials, d_moments);
     if (e == cudaSuccess) e = cudaMemcpyAsync(m, d_moments, sizeof(m), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -893,6 +893,19 @@ cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEven
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
+cudaError_t preload_noalloc_kernels() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, merge_tasks_kernel);
+    for (int model = 0; model < 2 && e == cudaSuccess; ++model)
+        for (int scheme = 0; scheme < 3 && e == cudaSuccess; ++scheme)
+            for (int trk = 0; trk < 2 && e == cudaSuccess; ++trk) {
+                e = cudaFuncGetAttributes(&fa, price_kernel_for<float>(model, scheme, true, kLaneOne, trk != 0));
+                if (e == cudaSuccess)
+                    e = cudaFuncGetAttributes(&fa, price_kernel_for<double>(model, scheme, true, kLaneOne, trk != 0));
+            }
+    return e;
+}
+
 int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode, bool track) {
     int nb = 0;
     if (precision == QK_FP32)

@@ -3,8 +3,9 @@
 Paths within a contract and contracts within a batch are independent, and every
 path's random numbers are keyed by (seed, stream, path, step) only, so a
 contract's price does not depend on which GPU prices it.  The data path needs no
-collective: each rank prices its shard with the batched engine; the only
-exchange is the per-contract results (a few hundred bytes each), gathered once.
+collective: each rank prices its shard with the batched engine on its own GPU;
+the only exchange is the per-contract results (a few hundred bytes each),
+gathered once.
 
 Sharding is greedy longest-processing-time on the path-step cost of each
 contract (with its Greek bumps), deterministic for a given contract list.
@@ -12,6 +13,7 @@ contract (with its Greek bumps), deterministic for a given contract list.
 from __future__ import annotations
 
 import heapq
+import os
 from typing import Callable, Sequence
 
 
@@ -33,13 +35,47 @@ def shard_contracts(contracts: Sequence, world: int, n_tasks: int = 1) -> list[l
     return shards
 
 
+def local_device() -> int:
+    """The GPU this process prices on: LOCAL_RANK when launched one process per GPU
+    (torchrun sets it), else torch's current CUDA device, else 0."""
+    lr = os.environ.get("LOCAL_RANK")
+    if lr is not None and lr.strip():
+        return int(lr)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return int(torch.cuda.current_device())
+    except Exception:
+        pass
+    return 0
+
+
+_rank_handles: dict = {}
+
+
+def rank_handle(device: int | None = None, factory: Callable | None = None):
+    """One engine handle per (process, device), created on first use and reused by
+    later sharded pricings.  `factory(device)` builds it (default: engine.Handle)."""
+    dev = local_device() if device is None else int(device)
+    key = (dev, factory)
+    h = _rank_handles.get(key)
+    if h is None:
+        if factory is None:
+            from .engine import Handle
+            factory = Handle
+        h = factory(dev)
+        _rank_handles[key] = h
+    return h
+
+
 def price_sharded(contracts: Sequence, greeks=None, group=None,
-                  pricer: Callable | None = None) -> list[dict] | None:
+                  pricer: Callable | None = None, handle_factory: Callable | None = None) -> list[dict] | None:
     """Price `contracts` across the ranks of `group` (torch.distributed, any backend).
 
     Every rank passes the same contract list.  Rank r prices shard r with `pricer`
-    (default: the batched engine on this rank's GPU) and rank 0 returns the results
-    in the original order; other ranks return None."""
+    (default: the batched engine on this rank's GPU, `local_device()`, through a
+    handle that `handle_factory(device)` builds once per process) and rank 0 returns
+    the results in the original order; other ranks return None."""
     import torch.distributed as dist
 
     world = dist.get_world_size(group)
@@ -51,8 +87,11 @@ def price_sharded(contracts: Sequence, greeks=None, group=None,
     shards = shard_contracts(contracts, world, n_tasks)
     mine = shards[rank]
     if pricer is None:
-        from .engine import price_batch
-        pricer = lambda cs, g: price_batch(cs, g)  # noqa: E731
+        handle = rank_handle(None, handle_factory)
+
+        def pricer(cs, g):
+            from .engine import price_batch
+            return price_batch(cs, g, handle)
     results = pricer([contracts[i] for i in mine], greeks) if mine else []
     gathered: list = [None] * world if rank == 0 else None
     dist.gather_object(list(zip(mine, results)), gathered, dst=0, group=group)

@@ -12,10 +12,10 @@
 * :func:`serving_stream` — Poisson arrivals of pricing requests drawn like the
   mixed batch with a 30% share of American puts.
 
-Choices the workload descriptions leave open are fixed here (and stated in
-DESIGN.md): S0 = 100, r = 0.03, q = 0; calls and puts 50/50; the barrier leg is an
-up-and-out call with B ~ U[1.15, 1.5] S0 or a down-and-out put with
-B ~ U[0.5, 0.85] S0; the binary leg is cash-or-nothing; Bates jumps
+Choices the workload descriptions leave open are fixed here: S0 = 100,
+r = 0.03, q = 0; calls and puts 50/50; the barrier leg is an up-and-out call
+with B ~ U[1.15, 1.5] S0 or a down-and-out put with B ~ U[0.5, 0.85] S0; the
+binary leg is cash-or-nothing; Bates jumps
 lambda ~ U[0.05, 0.5], muJ ~ U[-0.15, 0.05], sigmaJ ~ U[0.05, 0.2]; Greeks bump
 1% of S0, 1% of v0 (relative v0 bump, vega per unit of variance), 1 bp of r and
 one day (1/365) of T.

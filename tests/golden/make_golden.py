@@ -39,7 +39,7 @@ sys.path.insert(0, str(ROOT))
 
 from oracle import qkref as R  # noqa: E402
 
-REF = Path("/root/reference")
+from quantkos_b200.build import REFERENCE_ROOT as REF  # noqa: E402  (QK_REFERENCE_ROOT)
 
 PARAM_SETS = [
     # name, model params (Heston core + jumps), market r, q, dt

@@ -107,3 +107,57 @@ def _failing_worker(rank, world, port):
     except Exception:
         os._exit(3 if rank == 1 else 4)
     os._exit(0)
+
+
+class _FakeHandle:
+    def __init__(self, device):
+        self.device = device
+
+
+def _binding_worker(rank, world, port, q):
+    """Default pricer of price_sharded under one-process-per-GPU launch: the engine
+    entry point is replaced by a recorder, the handle factory by a fake, so the
+    test sees which device each rank's handle was built for without a GPU."""
+    import torch.distributed as dist
+
+    import quantkos_b200.engine as engine
+    from quantkos_b200.distributed import price_sharded, rank_handle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    os.environ["LOCAL_RANK"] = str(rank)
+    seen = []
+
+    def recording_price_batch(cs, g, handle):
+        seen.append(handle.device)
+        return _oracle_pricer(cs, g)
+
+    engine.price_batch = recording_price_batch
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res = price_sharded(_contracts(), None, None, None, _FakeHandle)
+        again = rank_handle(None, _FakeHandle)  # cached: the same handle on a second call
+        price_sharded(_contracts(), None, None, None, _FakeHandle)
+        payload = {"rank": rank, "devices": seen, "cached": rank_handle(None, _FakeHandle) is again}
+        gathered = [None] * world if rank == 0 else None
+        dist.gather_object(payload, gathered, dst=0)
+        if rank == 0:
+            q.put((gathered, [r["legs"][0]["price"] for r in res]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_default_pricer_binds_each_rank_to_its_local_gpu():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_binding_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    gathered, prices = q.get(timeout=240)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for entry in gathered:
+        assert entry["devices"] and all(d == entry["rank"] for d in entry["devices"])
+        assert entry["cached"]
+    assert prices == [r["legs"][0]["price"] for r in _oracle_pricer(_contracts(), None)]

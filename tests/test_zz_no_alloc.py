@@ -11,7 +11,8 @@ Checked through the C ABI: two calls in a row give the same prices as the
 regular batched entry point on the same contract (relative 1e-12: same kernel,
 same paths, only the tile merge order may differ), the shared array carries no
 state from one call into the next, and requests beyond the fixed size are
-rejected with a clear error.
+rejected with a clear error; and once the first call on the device (its set-up)
+has run, a further call leaves the device's free memory unchanged.
 """
 import ctypes as C
 
@@ -65,3 +66,22 @@ def test_noalloc_rejects_oversized_requests(qk, handle):
     k = qk.make_contract(payoffs=[qk.payoff(qk.AMERICAN, qk.PUT, 100.0)])
     st, _ = _call(qk, k)
     assert st == qk.lib.QK_ERR_UNSUPPORTED
+
+
+def test_noalloc_call_after_setup_allocates_no_device_memory(qk, handle):
+    """The property the entry point exists for: once the first call on the device
+    (its set-up) has run, another call leaves the device's free memory unchanged."""
+    import torch
+
+    torch.cuda.mem_get_info(0)  # torch's own CUDA state is set up before measuring
+    k = qk.make_contract(model=qk.HESTON, scheme=qk.ANDERSEN_QE, n_paths=2_000_000, n_steps=32, seed=99,
+                         precision=qk.FP32, payoffs=[qk.payoff(qk.EUROPEAN, qk.CALL, 100.0),
+                                                     qk.payoff(qk.ASIAN, qk.PUT, 95.0)])
+    st, first = _call(qk, k)  # set-up: loads the kernels and reserves the array on this device
+    assert st == qk.lib.QK_OK, qk.lib.lib().qk_last_error()
+    free_before, _ = torch.cuda.mem_get_info(0)
+    st, second = _call(qk, k)
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert st == qk.lib.QK_OK, qk.lib.lib().qk_last_error()
+    assert free_after == free_before
+    assert second.p[0].price == first.p[0].price and second.p[1].price == first.p[1].price
