@@ -454,6 +454,36 @@ static double payoff_of(const qk_payoff *ps, const PathOut *o, int n_steps, int 
     return x;
 }
 
+/* PayoffTracker on a fed spot sequence S_1..S_n (Payoff.hpp:84-160: the trackers start
+ * at S0, track_current_price after every step, evaluate_final_payoff at S_n): the same
+ * running sum / max / min updates as the path loop above, then payoff_of.  fp32: the
+ * sequence and the trackers in float, as the FP32 path loop keeps them. */
+int qko_payoff_path(const qk_payoff *ps, const double *S, int n, double S0, int fp32, double *out) {
+    if (n < 1 || !ps || !S || !out) return 1;
+    PathOut o;
+    double ssum = 0.0, smax = fp32 ? (double)(float)S0 : S0, smin = smax;
+    float smaxf = (float)S0, sminf = (float)S0;
+    for (int i = 0; i < n; ++i) {
+        if (fp32) {
+            const float s = (float)S[i];
+            ssum += (double)s;
+            smaxf = fmaxf(smaxf, s);
+            sminf = fminf(sminf, s);
+        } else {
+            ssum += S[i];
+            smax = fmax(smax, S[i]);
+            smin = fmin(smin, S[i]);
+        }
+    }
+    o.S = fp32 ? (double)(float)S[n - 1] : S[n - 1];
+    o.v = 0.0;
+    o.ssum = ssum;
+    o.smax = fp32 ? (double)smaxf : smax;
+    o.smin = fp32 ? (double)sminf : smin;
+    *out = payoff_of(ps, &o, n, fp32);
+    return 0;
+}
+
 /* Spot and variance paths (row-major count x n_steps, real units). */
 int qko_paths(const qk_contract *c, int64_t first, int64_t count, double *S_out, double *v_out) {
     qk_contract n;

@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
         L.qko_exact_call.argtypes = [C.c_int, C.POINTER(Contract), C.c_double, dp]
         L.qko_lsm_solve_reference.argtypes = [dp, dp, C.c_double, C.c_int, dp]
         L.qko_gl_nodes.argtypes = [dp, dp]
+        L.qko_payoff_path.argtypes = [C.POINTER(Payoff), dp, C.c_int, C.c_double, C.c_int, dp]
         _lib = L
     return _lib
 
@@ -126,6 +127,17 @@ def payoffs(contract, leg: int = 0) -> np.ndarray:
     out = np.empty(c.n_paths)
     lib().qko_payoffs(C.byref(c), leg, out.ctypes.data_as(C.POINTER(C.c_double)))
     return out
+
+
+def payoff_path(opt_type: int, right: int, S: np.ndarray, S0: float, K: float, B: float, fp32: bool = False) -> float:
+    """The oracle's payoff of one leg on a fed spot sequence S_1..S_n (trackers start at S0)."""
+    S = np.ascontiguousarray(S, dtype=np.float64)
+    ps = Payoff(opt_type, right, K, B)
+    out = C.c_double()
+    if lib().qko_payoff_path(C.byref(ps), S.ctypes.data_as(C.POINTER(C.c_double)), len(S), S0, int(fp32),
+                             C.byref(out)) != 0:
+        raise RuntimeError("qko_payoff_path failed")
+    return out.value
 
 
 def price(contract, greeks=None) -> dict:

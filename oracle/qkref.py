@@ -61,8 +61,21 @@ def lib(real_bytes: int = 8) -> C.CDLL:
         L.qkref_laguerre.argtypes = [C.c_double, C.c_int, dp]
         L.qkref_payoff.argtypes = [C.c_int, C.c_int, dp, C.c_int, C.c_double, C.c_double, C.c_double, dp]
         L.qkref_last_error.restype = C.c_char_p
+        L.qkref_set_threads.argtypes = [C.c_int]
+        L.qkref_get_threads.restype = C.c_int
         _libs[real_bytes] = L
     return _libs[real_bytes]
+
+
+def set_threads(n: int) -> None:
+    """Thread count of the reference's OpenMP loops in both builds.  Its generator pool
+    holds one state per thread, so a fixed count gives the same draws on any machine."""
+    for rb in (8, 4):
+        lib(rb).qkref_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib(8).qkref_get_threads())
 
 
 def config(**kw) -> RefConfig:

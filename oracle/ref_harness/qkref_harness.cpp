@@ -16,13 +16,16 @@
 //   qkref_exact_call   Black-Scholes / Heston / Bates closed forms
 //                      (include/core/analytical/{BlackScholes,Heston,Bates}Exact.hpp);
 //   qkref_lsm_solve / qkref_laguerre   LSMEngine pieces (include/core/options/LSMAmerican.hpp:157-613);
-//   qkref_payoff       PayoffTracker on a fed spot sequence (include/core/options/Payoff.hpp:84-243).
+//   qkref_payoff       PayoffTracker on a fed spot sequence (include/core/options/Payoff.hpp:84-243);
+//   qkref_set_threads  thread count of the shim's OpenMP loops (fixes the draw streams).
 #include <cstdint>
 #include <cstdio>
 #include <exception>
 #include <iostream>
 #include <sstream>
 #include <string>
+
+#include <omp.h>
 
 #include "core/schemes/RandNGenerator.hpp"
 
@@ -113,6 +116,14 @@ typedef struct {
 } qkref_result;
 
 int qkref_real_bytes(void) { return static_cast<int>(sizeof(KT::Real)); }
+
+// Threads of the shim's OpenMP loops.  The shim's generator pool has one state per
+// thread and the loops use a static schedule, so a fixed thread count makes the
+// reference's draws (and so its prices) the same on every machine.
+void qkref_set_threads(int n) {
+    if (n > 0) omp_set_num_threads(n);
+}
+int qkref_get_threads(void) { return omp_get_max_threads(); }
 }
 
 namespace {
