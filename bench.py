@@ -15,6 +15,12 @@ For N > 1 launch with torchrun (one process per GPU); every rank prices its own
 contract on its own Philox stream (weak scaling, no data-path collective); the
 timed region is bracketed by a barrier and device syncs and the max over ranks is
 reported.  Prints ONE JSON line on rank 0.
+
+At N = 1 the line also carries the other workloads, each with its own clock
+record: `batch_4096` (the 4096-contract mix with all seven Greeks, batched FP32
+engine against the plain FP64 drop-in on every contract) and `serve` /
+`serve_sub_capacity` (Poisson request streams at 2,000 and 1,000 requests/s, 30%
+American puts).  `--no-extra` leaves them out.
 """
 from __future__ import annotations
 
@@ -68,6 +74,11 @@ def parse_args():
                     help="bates5 (default): the headline line; the others measure the remaining workloads")
     ap.add_argument("--subset", type=int, default=128, help="batch: contracts priced by both engines")
     ap.add_argument("--requests", type=int, default=20_000, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="default line without the 4096-contract batch and serving records")
+    ap.add_argument("--batch-compare", type=int, default=4096,
+                    help="default line: contracts of the mix priced by both engines (4096 = all)")
     return ap.parse_args()
 
 
@@ -203,6 +214,163 @@ def _timed(torch, ext, fn, steps: int, flush=None) -> list[float]:
     return out
 
 
+def _shape_summary(tuned) -> list[dict]:
+    return [{k: r[k] for k in ("precision", "model", "scheme", "tiles_per_warp", "guided_tail", "paths_per_lane")}
+            for r in tuned]
+
+
+def _max_mhz() -> float:
+    pk = ROOT / "MEASURED_PEAKS.json"
+    return json.loads(pk.read_text()).get("sm_max_mhz", 1965.0) if pk.exists() else 1965.0
+
+
+def measure_batch_mix(qk, W, h, torch, ext, flush, subset: int | None = None, autotune: bool = True) -> dict:
+    """The 4096-contract mixed workload with all seven Greeks (49,152 pricing tasks):
+    one timed pricing by the batched FP32 engine (one persistent launch per kernel kind)
+    and one by the plain FP64 drop-in (one contract per launch sequence), on all the
+    contracts or the first `subset`, on the same Philox draws.  Reports contracts/s of
+    both, their ratio at equal standard error, the share of FP32 prices within 3 SE
+    of the FP64 ones, and the FP32-minus-FP64 Greeks in units of a conservative
+    finite-difference SE bound."""
+    g = W.batch_greeks()
+    full = W.mixed_batch()
+    n_cmp = len(full) if subset is None else min(subset, len(full))
+    tuned = h.autotune(full[:256], g, reps=1) if autotune else []  # launch shapes per kind (untimed)
+    cmp32 = full[:n_cmp]
+    cmp64 = W.mixed_batch(n_cmp, precision=qk.FP64)
+    qk.price_batch(cmp32[:64], g, h)
+    qk.price_plain(cmp64[0], g, h)
+    res32: list = []
+    res64: list = []
+    sampler = ClockSampler(0)
+    with sampler:
+        t_full = _timed(torch, ext, lambda: res32.__init__(qk.price_batch(full, g, h)), 1, flush)[0]
+        tf = h.last_timing()
+        if n_cmp < len(full):
+            t_cmp32 = _timed(torch, ext, lambda: res32.__init__(qk.price_batch(cmp32, g, h)), 1, flush)[0]
+        else:
+            t_cmp32 = t_full
+
+        def plain_all():
+            res64.clear()
+            for c in cmp64:
+                res64.append(qk.price_plain(c, g, h))
+
+        t_plain = _timed(torch, ext, plain_all, 1, flush)[0]
+    res32 = res32[:n_cmp]
+    se_ratio = statistics.mean(a["legs"][0]["std_error"] / b["legs"][0]["std_error"]
+                               for a, b in zip(res32, res64) if b["legs"][0]["std_error"] > 0)
+    dev = [abs(a["legs"][0]["price"] - b["legs"][0]["price"]) / b["legs"][0]["std_error"]
+           for a, b in zip(res32, res64) if b["legs"][0]["std_error"] > 0]
+    within = sum(d <= 3.0 for d in dev) / len(dev)
+
+    # Greeks: same draws on both sides, so the difference is precision, not sampling;
+    # in units of sd(X - Y) <= sd(X) + sd(Y) with every bumped price at the base SE
+    def se_bound(c, se, f):
+        hs = c.S0 * g.bump_S_rel
+        hv = c.v0 * g.bump_vol if g.vega_mode == 1 else g.bump_vol
+        return {"delta": se / hs, "gamma": 4 * se / hs ** 2, "vega": se / hv, "vomma": 4 * se / hv ** 2,
+                "vanna": se / (hs * hv), "rho": se / g.bump_r_abs, "theta": 2 * se / g.bump_T_abs}[f]
+
+    greek_err = {}
+    for f in ("delta", "gamma", "vega", "vomma", "vanna", "rho", "theta"):
+        rel, in_se = [], []
+        for c, a, b in zip(cmp64, res32, res64):
+            la, lb = a["legs"][0], b["legs"][0]
+            d = abs(la[f] - lb[f])
+            rel.append(d / max(abs(lb[f]), 1e-12))
+            bound = se_bound(c, lb["std_error"], f)
+            if bound > 0:
+                in_se.append(d / bound)
+        greek_err[f] = {"median_rel": statistics.median(rel), "median_in_se_bound": statistics.median(in_se),
+                        "max_in_se_bound": max(in_se)}
+    ps = W.path_steps(full, g)
+    batched_cps = n_cmp / (t_cmp32 * 1e-3)
+    plain_cps = n_cmp / (t_plain * 1e-3)
+    return {"workload": "mixed_4096_contracts_all_greeks_seed123", "contracts": len(full), "pricing_tasks": 12 * len(full),
+            "path_steps": ps, "batched_ms": t_full, "contracts_per_s": len(full) / (t_full * 1e-3),
+            "path_steps_per_s": ps / (t_full * 1e-3), "gpu_launches": tf["launches"],
+            "compared_contracts": n_cmp, "plain_fp64_ms": t_plain,
+            "batched_fp32_contracts_per_s": batched_cps, "plain_fp64_contracts_per_s": plain_cps,
+            "mean_se_ratio_batched_over_plain": se_ratio,
+            # contracts/s ratio at equal SE: the batched engine would need (SE ratio)^2 the paths
+            "speedup_vs_plain_fp64_at_equal_se": batched_cps / plain_cps / (se_ratio * se_ratio),
+            "prices_within_3se_of_fp64": within, "max_price_diff_in_fp64_se": max(dev),
+            "greeks_fp32_minus_fp64": greek_err, "autotune": _shape_summary(tuned),
+            "clocks": sampler.summary(_max_mhz())}
+
+
+def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, plain_sample: int = 0) -> dict:
+    """A Poisson stream of `n_requests` pricing requests at `rate` per second (30% American
+    puts by LSM) submitted in real time to the continuous-batching server started on h;
+    latency is submit to completion.  Optionally the plain FP64 one-contract-per-launch
+    method and the batched engine on the first `plain_sample` requests, for throughput
+    at equal standard error."""
+    import ctypes as C
+
+    from quantkos_b200 import _lib as L
+    import threading
+
+    arrivals, contracts = W.serving_stream(n_requests, rate_per_s=rate)
+    srv = qk.Server(h, 0, 512)
+    for c in contracts[:8]:  # both lanes warm
+        srv.poll(srv.submit(c), 600_000)
+    srv.stop()
+    srv = qk.Server(h, 0, 512)
+    tickets = []
+    sampler = ClockSampler(0)
+    t0 = time.perf_counter()
+
+    def producer():
+        for t_arr, c in zip(arrivals, contracts):
+            now = time.perf_counter() - t0
+            if t_arr > now:
+                time.sleep(t_arr - now)
+            tickets.append(srv.submit(c))
+
+    with sampler:
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        for tk in tickets:
+            while srv.poll(tk, 1000) is None:
+                pass
+    st = srv.stats()
+    srv.stop()
+    offered = W.path_steps(contracts)
+    rec = {"workload": f"serving_{n_requests}_requests_poisson_{rate:g}_per_s_30pct_american",
+           "rate_per_s": rate, "requests": n_requests, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+           "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "contracts_per_s": st["contracts_per_s"],
+           "path_steps_per_s": st["path_steps_per_s"], "offered_path_steps_per_s": offered / arrivals[-1],
+           "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
+           "clocks": sampler.summary(_max_mhz())}
+    if plain_sample:
+        sample = contracts[:plain_sample]
+        sample64 = []
+        for c in sample:
+            c64 = L.Contract()
+            C.memmove(C.byref(c64), C.byref(c), C.sizeof(L.Contract))
+            c64.precision = qk.FP64
+            sample64.append(c64)
+        qk.price_plain(sample64[0], None, h)
+        plain_res = []
+
+        def plain_all():
+            plain_res.clear()
+            for c in sample64:
+                plain_res.append(qk.price_plain(c, None, h))
+
+        t_plain = _timed(torch, ext, plain_all, 1, flush)[0]
+        batch_res = qk.price_batch(sample, None, h)
+        t_batch = _timed(torch, ext, lambda: qk.price_batch(sample, None, h), 1, flush)[0]
+        rec.update(sample=len(sample), sample_plain_fp64_contracts_per_s=len(sample) / (t_plain * 1e-3),
+                   sample_batched_contracts_per_s=len(sample) / (t_batch * 1e-3),
+                   sample_mean_se_ratio_batched_over_plain=statistics.mean(
+                       a["legs"][0]["std_error"] / b["legs"][0]["std_error"]
+                       for a, b in zip(batch_res, plain_res) if b["legs"][0]["std_error"] > 0))
+    return rec
+
+
 def run_other_workload(args) -> None:
     import ctypes as C
 
@@ -296,135 +464,22 @@ def run_other_workload(args) -> None:
                     gpu_launches=args.steps * t["launches"])
         line["roofline"]["frac"] = line["roofline"]["achieved"] / line["roofline"]["peak"]
     elif args.workload == "batch":
-        g = W.batch_greeks()
-        full = W.mixed_batch()
-        sub = full[:args.subset]
-        # launch shape per kernel kind from the autotuner on a sample of the batch (untimed)
-        tuned = [] if args.no_autotune else h.autotune(full[:256], g, reps=1)
-        sub64 = W.mixed_batch(args.subset, precision=qk.FP64)
-        qk.price_batch(sub, g, h)
-        t_sub = _timed(torch, ext, lambda: qk.price_batch(sub, g, h), 1, flush)[0]
-        res32 = qk.price_batch(sub, g, h)
-        qk.price_plain(sub64[0], g, h)
-        res64 = []
-
-        def plain_all():
-            res64.clear()
-            for c in sub64:
-                res64.append(qk.price_plain(c, g, h))
-
-        t_plain = _timed(torch, ext, plain_all, 1, flush)[0]
-        with sampler:
-            t_full = _timed(torch, ext, lambda: qk.price_batch(full, g, h), max(1, args.steps // 10), flush)
-        tf = h.last_timing()
-        ms = statistics.mean(t_full)
-        se_ratio = statistics.mean(a["legs"][0]["std_error"] / b["legs"][0]["std_error"]
-                                   for a, b in zip(res32, res64) if b["legs"][0]["std_error"] > 0)
-        within = sum(abs(a["legs"][0]["price"] - b["legs"][0]["price"]) <= 3.0 * b["legs"][0]["std_error"] + 1e-12
-                     for a, b in zip(res32, res64)) / len(sub)
-        # Greeks of the batched FP32 engine against the FP64 drop-in on the same draws (common
-        # random numbers): the difference is precision, not sampling.  Reported relative and in
-        # units of a conservative standard-error bound of each finite difference (sd(X - Y) <=
-        # sd(X) + sd(Y), every bumped price taken with the base price's standard error).
-        def se_bound(c, se, f):
-            hs = c.S0 * g.bump_S_rel
-            hv = c.v0 * g.bump_vol if g.vega_mode == 1 else g.bump_vol
-            return {"delta": se / hs, "gamma": 4 * se / hs ** 2, "vega": se / hv, "vomma": 4 * se / hv ** 2,
-                    "vanna": se / (hs * hv), "rho": se / g.bump_r_abs, "theta": 2 * se / g.bump_T_abs}[f]
-
-        greek_err = {}
-        for f in ("delta", "gamma", "vega", "vomma", "vanna", "rho", "theta"):
-            rel, in_se = [], []
-            for c, a, b in zip(sub64, res32, res64):
-                la, lb = a["legs"][0], b["legs"][0]
-                d = abs(la[f] - lb[f])
-                rel.append(d / max(abs(lb[f]), 1e-12))
-                bound = se_bound(c, lb["std_error"], f)
-                if bound > 0:
-                    in_se.append(d / bound)
-            greek_err[f] = {"median_rel": statistics.median(rel), "median_in_se_bound": statistics.median(in_se),
-                            "max_in_se_bound": max(in_se)}
-        line.update(metric="contracts/s", unit="contracts/s", value=len(full) / (ms * 1e-3), ms_per_step=ms,
-                    dtype="f32",
-                    config={"workload": "mixed_4096_contracts_all_greeks_seed123",
-                            "path_steps": W.path_steps(full, g), "path_steps_per_s": W.path_steps(full, g) / (ms * 1e-3),
-                            "subset": len(sub), "subset_batched_contracts_per_s": len(sub) / (t_sub * 1e-3),
-                            "subset_plain_fp64_contracts_per_s": len(sub) / (t_plain * 1e-3),
-                            "speedup_vs_plain_fp64_same_subset": t_plain / t_sub,
-                            "mean_se_ratio_batched_over_plain": se_ratio,
-                            "subset_prices_within_3se_of_fp64": within,
-                            "greeks_fp32_minus_fp64": greek_err,
-                            "autotune": [{k: r[k] for k in ("model", "scheme", "tiles_per_warp", "guided_tail",
-                                                            "paths_per_lane")} for r in tuned]},
-                    gpu_launches=tf["launches"])
+        rec = measure_batch_mix(qk, W, h, torch, ext, flush, subset=args.subset, autotune=not args.no_autotune)
+        ms = rec["batched_ms"]
+        line.update(metric="contracts/s", unit="contracts/s", value=rec["contracts_per_s"], ms_per_step=ms,
+                    dtype="f32", config=rec, gpu_launches=rec["gpu_launches"])
+        sampler = None
     else:  # serve
-        arrivals, contracts = W.serving_stream(args.requests)
-        # launch shapes per kernel kind from the autotuner on a sample of the stream
-        # (untimed); the server's lanes take them from h
+        _, contracts = W.serving_stream(256)
         tuned = [] if args.no_autotune else h.autotune(contracts[:256], None, reps=1)
-        srv = qk.Server(h, 0, 512)
-        # warm both lanes
-        for c in contracts[:8]:
-            srv.poll(srv.submit(c), 600_000)
-        srv.stop()
-        srv = qk.Server(h, 0, 512)
-        import threading
-        tickets = []
-        t0 = time.perf_counter()
-
-        def producer():
-            for t_arr, c in zip(arrivals, contracts):
-                now = time.perf_counter() - t0
-                if t_arr > now:
-                    time.sleep(t_arr - now)
-                tickets.append(srv.submit(c))
-
-        with sampler:
-            th = threading.Thread(target=producer)
-            th.start()
-            th.join()
-            for tk in tickets:
-                while srv.poll(tk, 1000) is None:
-                    pass
-        st = srv.stats()
-        srv.stop()
-        offered = W.path_steps(contracts)
-        # the plain FP64 one-contract-per-launch method on a sample of the same requests
-        sample = contracts[:args.subset]
-        sample64 = []
-        for c in sample:
-            c64 = L.Contract()
-            C.memmove(C.byref(c64), C.byref(c), C.sizeof(L.Contract))
-            c64.precision = qk.FP64
-            sample64.append(c64)
-        qk.price_plain(sample64[0], None, h)
-        plain_res = []
-
-        def plain_all():
-            plain_res.clear()
-            for c in sample64:
-                plain_res.append(qk.price_plain(c, None, h))
-
-        t_plain = _timed(torch, ext, plain_all, 1, flush)[0]
-        batch_res = qk.price_batch(sample, None, h)
-        t_batch = _timed(torch, ext, lambda: qk.price_batch(sample, None, h), 1, flush)[0]
-        se_ratio = statistics.mean(a["legs"][0]["std_error"] / b["legs"][0]["std_error"]
-                                   for a, b in zip(batch_res, plain_res) if b["legs"][0]["std_error"] > 0)
-        line.update(metric="contracts/s", unit="contracts/s", value=st["contracts_per_s"], dtype="f32",
-                    ms_per_step=None,
-                    config={"workload": f"serving_{args.requests}_requests_poisson_2000_per_s_30pct_american",
-                            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"],
-                            "max_ms": st["max_ms"], "path_steps_per_s": st["path_steps_per_s"],
-                            "offered_path_steps": offered, "offered_path_steps_per_s": offered / arrivals[-1],
-                            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
-                            "sample": len(sample), "sample_plain_fp64_contracts_per_s": len(sample) / (t_plain * 1e-3),
-                            "sample_batched_contracts_per_s": len(sample) / (t_batch * 1e-3),
-                            "sample_mean_se_ratio_batched_over_plain": se_ratio,
-                            "autotune": [{k: r[k] for k in ("model", "scheme", "tiles_per_warp", "guided_tail",
-                                                            "paths_per_lane")} for r in tuned]},
-                    gpu_launches=None)
+        rec = measure_serving(qk, W, h, torch, ext, flush, rate=args.rate, n_requests=args.requests,
+                              plain_sample=args.subset)
+        rec["autotune"] = _shape_summary(tuned)
+        line.update(metric="contracts/s", unit="contracts/s", value=rec["contracts_per_s"], dtype="f32",
+                    ms_per_step=None, config=rec, gpu_launches=None)
+        sampler = None
     pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    line["clocks"] = sampler.summary(pk.get("sm_max_mhz", 1965.0))
+    line["clocks"] = sampler.summary(pk.get("sm_max_mhz", 1965.0)) if sampler else line["config"].pop("clocks")
     print(json.dumps(line), flush=True)
     h.close()
 
@@ -639,6 +694,16 @@ def main() -> None:
             "clocks": clocks,
             "gpu_launches": launches,
         }
+        if world == 1 and not args.no_extra:
+            # the other north-star workloads, each with its own clock record: the 4096-contract
+            # mix with all Greeks against the plain FP64 drop-in, and the serving stream at
+            # 2,000 requests/s (over capacity) and at 1,000 requests/s (under it)
+            from quantkos_b200 import workloads as W
+            line["batch_4096"] = measure_batch_mix(qk, W, h, torch, ext, flush,
+                                                   subset=args.batch_compare, autotune=not args.no_autotune)
+            line["serve"] = measure_serving(qk, W, h, torch, ext, flush, rate=2000.0, n_requests=20_000)
+            line["serve_sub_capacity"] = measure_serving(qk, W, h, torch, ext, flush, rate=1000.0,
+                                                         n_requests=10_000)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
