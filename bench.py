@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -49,6 +50,28 @@ METRIC = "path-steps/s"
 # at (measured SFU op rate) / 12 path-steps/s; the FP32/integer work (Philox, the
 # QE algebra) fits under that bound on the 128-lane issue.
 SFU_PER_STEP = 12.0
+# Algorithmic scalar lane operations per path-step of the FP32 kinds (from the formulas
+# as implemented; one-path-per-lane count), for the issue-slot bound (every operation,
+# SFU ones included, takes an issue slot; an SM issues 4 warp instructions = 128 lane
+# operations per cycle, 8 times its 16 SFU lanes):
+#   Philox4x32-10: half a call per step (a call = 4 words = two steps' normal pairs):
+#     10 rounds x (2 wide multiplies + 2 three-input XORs) / 2 = 20
+#   Box-Muller per pair: 2 uniform conversions x 2, the log and angle scalings, 2 products
+#     = 8 (+ 4 SFU: lg2, sqrt, sin, cos)
+#   step: Euler 10 (+2 SFU: sqrt v, ex2), Milstein 14 (+2), QE quadratic 30 (+8: 3 rcp,
+#     3 sqrt, lg2, ex2)
+#   Bates: the one-compare jump test, 5; loop and counters, 3
+ISSUE_OPS = {"philox": 20, "box_muller": 8, "step": {"euler": 10, "milstein": 14, "qe": 30}, "bates": 5, "loop": 3}
+SFU_OPS = {"box_muller": 4, "step": {"euler": 2, "milstein": 2, "qe": 8}}
+
+
+def algorithmic_ops(scheme: str, bates: bool) -> tuple[int, int]:
+    """(SFU operations, issue-slot operations incl. SFU) per path-step of one FP32 kind."""
+    sfu = SFU_OPS["box_muller"] + SFU_OPS["step"][scheme]
+    other = ISSUE_OPS["philox"] + ISSUE_OPS["box_muller"] + ISSUE_OPS["step"][scheme] + ISSUE_OPS["loop"]
+    if bates:
+        other += ISSUE_OPS["bates"]
+    return sfu, sfu + other
 DRAM_BYTES_PER_PATH_STEP = 2.09e6 / (1_048_576 * 252)
 L2_FLUSH_BYTES = 256 << 20
 
@@ -75,6 +98,8 @@ def parse_args():
     ap.add_argument("--subset", type=int, default=128, help="batch: contracts priced by both engines")
     ap.add_argument("--requests", type=int, default=20_000, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--lanes", type=int, default=0, help="serve: server lanes (0 = the library default)")
+    ap.add_argument("--wave-ms", type=float, default=0.0, help="serve: wave budget in ms (0 = the library default)")
     ap.add_argument("--no-extra", action="store_true",
                     help="default line without the 4096-contract batch and serving records")
     ap.add_argument("--batch-compare", type=int, default=4096,
@@ -263,6 +288,16 @@ def measure_batch_mix(qk, W, h, torch, ext, flush, subset: int | None = None, au
     dev = [abs(a["legs"][0]["price"] - b["legs"][0]["price"]) / b["legs"][0]["std_error"]
            for a, b in zip(res32, res64) if b["legs"][0]["std_error"] > 0]
     within = sum(d <= 3.0 for d in dev) / len(dev)
+    # Heston contracts follow the same paths in both precisions (the difference is rounding);
+    # under Bates the FP32 jump decision reads other bits than the FP64 one, so jump times
+    # differ and the two estimates are partly independent: compared in combined SE
+    comb = {"heston": [], "bates": []}
+    for c, a, b in zip(cmp64, res32, res64):
+        la, lb = a["legs"][0], b["legs"][0]
+        s = math.hypot(la["std_error"], lb["std_error"])
+        if s > 0:
+            comb["bates" if c.model == qk.BATES else "heston"].append(abs(la["price"] - lb["price"]) / s)
+    all_comb = comb["heston"] + comb["bates"]
 
     # Greeks: same draws on both sides, so the difference is precision, not sampling;
     # in units of sd(X - Y) <= sd(X) + sd(Y) with every bumped price at the base SE
@@ -296,11 +331,14 @@ def measure_batch_mix(qk, W, h, torch, ext, flush, subset: int | None = None, au
             # contracts/s ratio at equal SE: the batched engine would need (SE ratio)^2 the paths
             "speedup_vs_plain_fp64_at_equal_se": batched_cps / plain_cps / (se_ratio * se_ratio),
             "prices_within_3se_of_fp64": within, "max_price_diff_in_fp64_se": max(dev),
+            "prices_within_3_combined_se": sum(d <= 3.0 for d in all_comb) / len(all_comb),
+            "max_price_diff_in_combined_se": {k: max(v) if v else None for k, v in comb.items()},
             "greeks_fp32_minus_fp64": greek_err, "autotune": _shape_summary(tuned),
             "clocks": sampler.summary(_max_mhz())}
 
 
-def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, plain_sample: int = 0) -> dict:
+def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, plain_sample: int = 0,
+                    lanes: int = 0, wave_ms: float = 0.0) -> dict:
     """A Poisson stream of `n_requests` pricing requests at `rate` per second (30% American
     puts by LSM) submitted in real time to the continuous-batching server started on h;
     latency is submit to completion.  Optionally the plain FP64 one-contract-per-launch
@@ -312,11 +350,11 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
     import threading
 
     arrivals, contracts = W.serving_stream(n_requests, rate_per_s=rate)
-    srv = qk.Server(h, 0, 512)
-    for c in contracts[:8]:  # both lanes warm
+    srv = qk.Server(h, 0, 512, lanes, wave_ms)
+    for c in contracts[:16]:  # the lanes warm
         srv.poll(srv.submit(c), 600_000)
     srv.stop()
-    srv = qk.Server(h, 0, 512)
+    srv = qk.Server(h, 0, 512, lanes, wave_ms)
     tickets = []
     sampler = ClockSampler(0)
     t0 = time.perf_counter()
@@ -338,11 +376,18 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
     st = srv.stats()
     srv.stop()
     offered = W.path_steps(contracts)
+    # the ceiling: the batched engine pricing every request of the stream in one call
+    qk.price_batch(contracts[:64], None, h)
+    t_all = _timed(torch, ext, lambda: qk.price_batch(contracts, None, h), 1, flush)[0]
     rec = {"workload": f"serving_{n_requests}_requests_poisson_{rate:g}_per_s_30pct_american",
            "rate_per_s": rate, "requests": n_requests, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
            "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "contracts_per_s": st["contracts_per_s"],
            "path_steps_per_s": st["path_steps_per_s"], "offered_path_steps_per_s": offered / arrivals[-1],
            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
+           "lanes": lanes or 4, "wave_ms": wave_ms or 8.0,
+           "batch_all_contracts_per_s": n_requests / (t_all * 1e-3),
+           "batch_all_path_steps_per_s": offered / (t_all * 1e-3),
+           "served_over_batch_all": st["contracts_per_s"] / (n_requests / (t_all * 1e-3)),
            "clocks": sampler.summary(_max_mhz())}
     if plain_sample:
         sample = contracts[:plain_sample]
@@ -406,10 +451,12 @@ def run_other_workload(args) -> None:
         # path-kernel time against each kind's SFU bound (Euler and Milstein: Box-Muller
         # lg2, sqrt, sin, cos + sqrt(v), ex2 = 6 ops per path-step; QE: 12)
         sfu_ops = h.measure_sfu()
+        issue_ops = 8.0 * sfu_ops  # lane operations per second the SMs can issue (128 vs 16 per cycle)
         kinds, total = [], 0.0
         with sampler:
             for model in (qk.HESTON, qk.BATES):
-                for scheme, n_sfu in ((qk.EULER, 6), (qk.IMPLICIT_MILSTEIN, 6), (qk.ANDERSEN_QE, 12)):
+                for scheme, sname in ((qk.EULER, "euler"), (qk.IMPLICIT_MILSTEIN, "milstein"), (qk.ANDERSEN_QE, "qe")):
+                    n_sfu, n_issue = algorithmic_ops(sname, model == qk.BATES)
                     c = qk.make_contract(S0=100.0, v0=0.04, r=0.03, q=0.0, model=model, scheme=scheme, kappa=2.0,
                                          theta=0.04, sigma=0.3, rho=-0.7,
                                          lambda_j=0.1 if model == qk.BATES else 0.0, mu_j=-0.05, sigma_j=0.10,
@@ -427,14 +474,17 @@ def run_other_workload(args) -> None:
                     k_ms = statistics.mean(ms)
                     ps = N_PATHS * N_STEPS / (k_ms * 1e-3)
                     total += k_ms
-                    kinds.append({"model": "bates" if model == qk.BATES else "heston",
-                                  "scheme": {qk.EULER: "euler", qk.IMPLICIT_MILSTEIN: "milstein",
-                                             qk.ANDERSEN_QE: "qe"}[scheme],
+                    sfu_frac = ps / (sfu_ops / n_sfu)
+                    issue_frac = ps / (issue_ops / n_issue)
+                    kinds.append({"model": "bates" if model == qk.BATES else "heston", "scheme": sname,
                                   "kernel_ms": k_ms, "gpath_steps_per_s": ps / 1e9, "sfu_ops_per_step": n_sfu,
-                                  "frac_of_sfu_bound": ps / (sfu_ops / n_sfu)})
+                                  "issue_ops_per_step": n_issue, "frac_of_sfu_bound": sfu_frac,
+                                  "frac_of_issue_bound": issue_frac, "frac": max(sfu_frac, issue_frac),
+                                  "bound": "sfu" if sfu_frac >= issue_frac else "issue"})
         line.update(value=6 * N_PATHS * N_STEPS / (total * 1e-3), ms_per_step=total / 6, dtype="f32",
                     config={"workload": f"fp32_kernel_kinds_european_{N_PATHS}x{N_STEPS}", "kinds": kinds,
-                            "sfu_ops_per_s": sfu_ops},
+                            "sfu_ops_per_s": sfu_ops, "issue_lane_ops_per_s": issue_ops,
+                            "algorithmic_ops": {"issue": ISSUE_OPS, "sfu": SFU_OPS}},
                     gpu_launches=None)
     elif args.workload == "lsm":
         c32 = W.american_lsm(precision=qk.FP32)
@@ -473,7 +523,7 @@ def run_other_workload(args) -> None:
         _, contracts = W.serving_stream(256)
         tuned = [] if args.no_autotune else h.autotune(contracts[:256], None, reps=1)
         rec = measure_serving(qk, W, h, torch, ext, flush, rate=args.rate, n_requests=args.requests,
-                              plain_sample=args.subset)
+                              plain_sample=args.subset, lanes=args.lanes, wave_ms=args.wave_ms)
         rec["autotune"] = _shape_summary(tuned)
         line.update(metric="contracts/s", unit="contracts/s", value=rec["contracts_per_s"], dtype="f32",
                     ms_per_step=None, config=rec, gpu_launches=None)

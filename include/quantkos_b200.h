@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define QK_ABI_VERSION 1
+#define QK_ABI_VERSION 2
 #define QK_MAX_PAYOFFS 8
 
 /* ---------------------------------------------------------------- status */
@@ -215,17 +215,21 @@ typedef struct qk_tune_report {
     double best_ms[QK_TUNE_KINDS];           /* device time of pricing the sample's tasks of this kind, chosen shape */
     double default_ms[QK_TUNE_KINDS];        /* the same with the defaults */
     int32_t candidates;                      /* shapes timed per kind */
+    int32_t block_size[QK_TUNE_KINDS];       /* chosen: threads per block of the pricing kernel */
 } qk_tune_report;
 
 /* Times the sample `c` (forward contracts; American ones are skipped) kind by
  * kind under every candidate shape (tiles per warp slot 4, 8, 12, 24, 48; tail
- * off, on; 1 or 2 paths per lane), `reps` timed runs each after one warm-up, keeps the fastest shape per kind
+ * off, on; 1 or 2 paths per lane), then the threads per block (128, 256, 512; FP64
+ * 128, 256) at the best of those, `reps` timed runs each after one warm-up, keeps the fastest shape per kind
  * in the handle for later qk_price_batch / qk_batch_prepare calls and reports it.
  * Prices do not depend on the shape beyond the last bits of the moment merge. */
 qk_status qk_autotune(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *g, int32_t reps,
                       qk_tune_report *out);
-/* Restores the default shape of every kind. */
+/* Restores the default shape of every kind (256 threads per block). */
 qk_status qk_tune_reset(qk_handle *h);
+/* Threads per block of one kind's pricing kernel: 128, 256 or 512 (FP64: 128 or 256). */
+qk_status qk_tune_set_block(qk_handle *h, int32_t precision, int32_t model, int32_t scheme, int32_t threads_per_block);
 /* Sets one kind's shape by hand (for example a stored autotuner result). */
 qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t scheme, int32_t tiles_per_warp,
                       int32_t guided_tail, int32_t paths_per_lane);
@@ -250,6 +254,15 @@ qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t sc
  * stream); the call returns after its work has finished. */
 qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_result *out);
 
+/* ---------------------------------------------------------------- failure-path testing
+ * qk_debug_lsm_withhold_block — no counterpart in the reference.  The backward
+ * induction of an American job runs as one launch whose blocks wait, with a bound of
+ * about a second, for each exercise date's coefficients.  With block >= 0, block
+ * `block` of every later backward launch on h leaves before its first arrival, so
+ * the other blocks' waits run out: the pricing call returns QK_ERR_TIMEOUT and the
+ * device stays usable.  block < 0 restores normal operation.  For tests only. */
+qk_status qk_debug_lsm_withhold_block(qk_handle *h, int32_t block);
+
 /* ---------------------------------------------------------------- parity harness
  * qk_step_trace — SDEScheme<M,S>::evolve_step with fed draws
  * (include/core/schemes/markovian/MSchemes.hpp:133-156, 229-253, 363-442, 493-526),
@@ -265,6 +278,44 @@ qk_status qk_step_trace(int32_t precision, const qk_contract *c, const double *z
  * (the .paths payload layout, include/IO/IOBinary.hpp:96-249), FP64 output. */
 qk_status qk_paths_dump(qk_handle *h, const qk_contract *c, int64_t first, int64_t count, double *S_out,
                         double *v_out);
+
+/* ---------------------------------------------------------------- engine pieces
+ * The building blocks the reference's C++ engine exposes, run by the same device code
+ * the fused kernels use (the C++ wrappers in quantkos_b200.hpp carry the reference's
+ * names).  They serve tests, parity checks and callers that drive the steps themselves;
+ * the pricing entry points above do not go through them.
+ *
+ * qk_payoff_trace — PayoffTracker<T,R> (include/core/options/Payoff.hpp:84-243):
+ * track_current_price over S[0..n-1] starting from S0, then evaluate_final_payoff at
+ * S[n-1] with leg->strike and leg->barrier, in `precision` (qk_precision). */
+qk_status qk_payoff_trace(const qk_payoff *leg, const double *S, int32_t n, double S0, int32_t precision,
+                          double *payoff);
+/* qk_payoffs_range — the per-path payoffs of one batch of paths as
+ * MSolver<M,S,T,R>::execute_batch writes them (include/core/schemes/markovian/MSolver.hpp:195-232):
+ * leg 0 of paths [first, first + count) of contract c, undiscounted, in normalised
+ * units when c->normalize (the OptionPricer rescales), the same paths the pricing
+ * kernels simulate. */
+qk_status qk_payoffs_range(qk_handle *h, const qk_contract *c, int64_t first, int64_t count, double *payoffs);
+/* qk_lsm_date — one exercise date of LSMEngine<R,Basis> on n caller paths
+ * (include/core/options/LSMAmerican.hpp:252-335): op 0 initialize_cashflows (cf =
+ * intrinsic(S)); op 1 perform_cross_paths_regression (sums over in-the-money paths with
+ * Y = cf * disc, then the FP64 solve into coeffs[4 or 6], *method 0 Cholesky, 1 pivoted
+ * QR, 2 mean fallback); op 2 update_cashflows (exercise iff intrinsic beats the
+ * continuation of coeffs, else cf * disc).  S and K in the units of the contract (S/K is
+ * what the basis sees); v (variance) only for QK_LSM_POLY_SV, whose basis is centred at
+ * (cx, cv).  precision: arithmetic of the path values, as the sweep kernel. */
+qk_status qk_lsm_date(int32_t op, int32_t precision, int32_t basis, int32_t right, int64_t n, const double *S,
+                      const double *v, double *cf, double K, double disc, double cx, double cv, double *coeffs,
+                      int32_t *method);
+/* qk_lsm_solve — LSMEngine::solve_system_on_host_cholesky (LSMAmerican.hpp:516-613) for
+ * QK_LSM_LAGUERRE3, the scaled Cholesky / pivoted QR for QK_LSM_POLY_SV: sums = upper
+ * Gram row-major, right-hand side, count (15 or 28 values). */
+qk_status qk_lsm_solve(int32_t basis, const double *sums, double *coeffs, int32_t *method);
+/* qk_paths_write — BinWriter (include/IO/IOBinary.hpp:72-249) on host arrays, no device
+ * involved: the header and n_paths x n_steps spot values given in real units, row-major,
+ * stored normalised (divided by `scale`) in `precision`, as qk_run_config writes them. */
+qk_status qk_paths_write(const char *path, int32_t precision, int64_t n_paths, int32_t n_steps, double dt,
+                         double scale, const double *S);
 
 /* ---------------------------------------------------------------- configuration
  * qk_config mirrors quantkos::Config::UInputs (include/core/config/Config.hpp:677-775)
@@ -317,10 +368,11 @@ qk_status qk_run_config(qk_handle *h, const qk_config *c, qk_result *out, double
 
 /* ---------------------------------------------------------------- serving
  * A continuous-batching request loop.  Requests are admitted by the HBM their
- * LSM slabs and partials need (budget in MiB; 0 = 80% of free HBM), batched with
- * whatever else has arrived, and their results polled by ticket.  The lanes use
- * h's device and the launch shapes h holds when the server starts (defaults, or
- * those set by qk_autotune / qk_tune_set). */
+ * LSM slabs and partials need (budget in MiB; 0 = 80% of free HBM) into waves of a
+ * few milliseconds of estimated GPU time, batched with whatever else has arrived;
+ * several lanes' waves run on the GPU at once; results are polled by ticket.  The
+ * lanes use h's device and the launch shapes h holds when the server starts
+ * (defaults, or those set by qk_autotune / qk_tune_set). */
 typedef struct qk_server qk_server;
 typedef struct qk_serve_stats {
     int64_t submitted, completed, rejected;
@@ -330,6 +382,19 @@ typedef struct qk_serve_stats {
     double busy_s;
 } qk_serve_stats;
 qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch, qk_server **out);
+/* The same with all options: lanes = host threads, each with its own handle and stream,
+ * whose waves run on the GPU at the same time (0 = 4); wave_ms = estimated GPU time at
+ * which a lane closes the wave it is admitting, raised to the lane's share of the
+ * waiting requests' estimated time when that is larger (0 = 8 ms; a wave always takes
+ * at least one request); hbm_budget_mib and max_batch as above.  qk_serve_start uses
+ * the defaults for lanes and wave_ms. */
+typedef struct qk_serve_options {
+    int64_t hbm_budget_mib;
+    int32_t max_batch;
+    int32_t lanes;
+    double wave_ms;
+} qk_serve_options;
+qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server **out);
 qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g, int64_t *ticket);
 /* done = 1 and *out filled once the ticket finished; wait_ms bounds the wait (0 = poll). */
 qk_status qk_serve_poll(qk_server *s, int64_t ticket, int32_t wait_ms, int32_t *done, qk_result *out);

@@ -62,6 +62,7 @@ def lib(real_bytes: int = 8) -> C.CDLL:
         L.qkref_payoff.argtypes = [C.c_int, C.c_int, dp, C.c_int, C.c_double, C.c_double, C.c_double, dp]
         L.qkref_last_error.restype = C.c_char_p
         L.qkref_set_threads.argtypes = [C.c_int]
+        L.qkref_read_paths.argtypes = [C.c_char_p, C.c_char_p, C.c_double, dp, C.c_int, C.POINTER(C.c_int)]
         L.qkref_get_threads.restype = C.c_int
         _libs[real_bytes] = L
     return _libs[real_bytes]
@@ -158,3 +159,14 @@ def payoff(opt_type: int, right: int, S: np.ndarray, S0: float, K: float, B: flo
     if rc != 0:
         raise RuntimeError("qkref_payoff")
     return out.value
+
+
+def read_paths(directory: str, filename: str, t: float, max_n: int, real_bytes: int = 8) -> np.ndarray:
+    """The reference's BinReader: every path's spot at time t (real units) from a .paths file."""
+    out = np.empty(max_n)
+    n = C.c_int()
+    rc = lib(real_bytes).qkref_read_paths(directory.encode(), filename.encode(), t,
+                                          out.ctypes.data_as(C.POINTER(C.c_double)), max_n, C.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"qkref_read_paths: {lib(real_bytes).qkref_last_error().decode()}")
+    return out[:n.value]

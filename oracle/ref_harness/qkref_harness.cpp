@@ -17,7 +17,9 @@
 //                      (include/core/analytical/{BlackScholes,Heston,Bates}Exact.hpp);
 //   qkref_lsm_solve / qkref_laguerre   LSMEngine pieces (include/core/options/LSMAmerican.hpp:157-613);
 //   qkref_payoff       PayoffTracker on a fed spot sequence (include/core/options/Payoff.hpp:84-243);
-//   qkref_set_threads  thread count of the shim's OpenMP loops (fixes the draw streams).
+//   qkref_set_threads  thread count of the shim's OpenMP loops (fixes the draw streams);
+//   qkref_read_paths   BinReader::read_prices_at_target_time on a .paths file
+//                      (include/IO/IOBinary.hpp:260-378).
 #include <cstdint>
 #include <cstdio>
 #include <exception>
@@ -81,6 +83,7 @@ struct NormalPair<FeedRNG &, skip_second> {
 #include "core/options/LSMAmerican.hpp"
 #include "core/options/Payoff.hpp"
 #include "core/schemes/markovian/MSchemes.hpp"
+#include "IO/IOBinary.hpp"
 
 namespace KC = quantkos::Config;
 namespace KE = quantkos::Engine;
@@ -358,5 +361,24 @@ extern "C" int qkref_payoff(int type, int right, const double *S, int n, double 
         case KI::OptType::BinaryCashOrNothing: *out = payoff_right<KI::OptType::BinaryCashOrNothing>(right, S, n, S0, K, B); return 0;
         case KI::OptType::BinaryAssetOrNothing: *out = payoff_right<KI::OptType::BinaryAssetOrNothing>(right, S, n, S0, K, B); return 0;
         default: return 1;
+    }
+}
+
+// BinReader (include/IO/IOBinary.hpp:260-378) on `dir`/`file`: the spot prices of every
+// path at time t, in real units (the reader rescales the stored normalised values).
+extern "C" int qkref_read_paths(const char *dir, const char *file, double t, double *out, int max_n, int *n_out) {
+    try {
+        KC::UInputs cfg;
+        cfg.output.out_dir = dir;
+        cfg.output.filename_paths_out = file;
+        quantkos::IO::Binary::BinReader reader(cfg);
+        const auto v = reader.read_prices_at_target_time(static_cast<KT::Real>(t));
+        const int n = static_cast<int>(v.size());
+        *n_out = n;
+        for (int i = 0; i < n && i < max_n; ++i) out[i] = static_cast<double>(v[i]);
+        return 0;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return 2;
     }
 }

@@ -87,7 +87,8 @@ class TuneReport(C.Structure):
                 ("scheme", C.c_int32 * TUNE_KINDS), ("tiles_per_warp", C.c_int32 * TUNE_KINDS),
                 ("guided_tail", C.c_int32 * TUNE_KINDS), ("paths_per_lane", C.c_int32 * TUNE_KINDS),
                 ("best_ms", C.c_double * TUNE_KINDS),
-                ("default_ms", C.c_double * TUNE_KINDS), ("candidates", C.c_int32)]
+                ("default_ms", C.c_double * TUNE_KINDS), ("candidates", C.c_int32),
+                ("block_size", C.c_int32 * TUNE_KINDS)]
 
 
 class ServeStats(C.Structure):
@@ -118,6 +119,10 @@ class Config(C.Structure):
     ]
 
 
+class ServeOptions(C.Structure):
+    _fields_ = [("hbm_budget_mib", C.c_int64), ("max_batch", C.c_int32), ("lanes", C.c_int32), ("wave_ms", C.c_double)]
+
+
 _P = C.POINTER
 _VP = C.c_void_p
 
@@ -131,6 +136,7 @@ SIGNATURES = {
     "qk_last_timing": (C.c_int, [_VP, _P(Timing)]),
     "qk_autotune": (C.c_int, [_VP, _P(Contract), C.c_int32, _P(Greeks), C.c_int32, _P(TuneReport)]),
     "qk_tune_set": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "qk_tune_set_block": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "qk_tune_reset": (C.c_int, [_VP]),
     "qk_measure_sfu": (C.c_int, [_VP, _P(C.c_double)]),
     "qk_validate": (C.c_int, [_P(Contract), _P(Greeks)]),
@@ -140,6 +146,15 @@ SIGNATURES = {
     "qk_batch_run": (C.c_int, [_VP]),
     "qk_batch_fetch": (C.c_int, [_VP, _P(Result), C.c_int32]),
     "qk_price_noalloc": (C.c_int, [_P(Contract), _VP, _P(Result)]),
+    "qk_debug_lsm_withhold_block": (C.c_int, [_VP, C.c_int32]),
+    "qk_payoff_trace": (C.c_int, [_P(Payoff), _P(C.c_double), C.c_int32, C.c_double, C.c_int32, _P(C.c_double)]),
+    "qk_payoffs_range": (C.c_int, [_VP, _P(Contract), C.c_int64, C.c_int64, _P(C.c_double)]),
+    "qk_lsm_date": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64, _P(C.c_double),
+                              _P(C.c_double), _P(C.c_double), C.c_double, C.c_double, C.c_double, C.c_double,
+                              _P(C.c_double), _P(C.c_int32)]),
+    "qk_lsm_solve": (C.c_int, [C.c_int32, _P(C.c_double), _P(C.c_double), _P(C.c_int32)]),
+    "qk_paths_write": (C.c_int, [C.c_char_p, C.c_int32, C.c_int64, C.c_int32, C.c_double, C.c_double,
+                                 _P(C.c_double)]),
     "qk_step_trace": (C.c_int, [C.c_int32, _P(Contract), _P(C.c_double), _P(C.c_double), C.c_int32, C.c_int32,
                                 _P(C.c_double), _P(C.c_double)]),
     "qk_paths_dump": (C.c_int, [_VP, _P(Contract), C.c_int64, C.c_int64, _P(C.c_double), _P(C.c_double)]),
@@ -150,6 +165,7 @@ SIGNATURES = {
     "qk_config_to_contract": (C.c_int, [_P(Config), _P(Contract), _P(Greeks)]),
     "qk_run_config": (C.c_int, [_VP, _P(Config), _P(Result), _P(C.c_double)]),
     "qk_serve_start": (C.c_int, [_VP, C.c_int64, C.c_int32, _P(_VP)]),
+    "qk_serve_start_ex": (C.c_int, [_VP, _P(ServeOptions), _P(_VP)]),
     "qk_serve_submit": (C.c_int, [_VP, _P(Contract), _P(Greeks), _P(C.c_int64)]),
     "qk_serve_poll": (C.c_int, [_VP, C.c_int64, C.c_int32, _P(C.c_int32), _P(Result)]),
     "qk_serve_cancel": (C.c_int, [_VP, C.c_int64, _P(C.c_int32)]),

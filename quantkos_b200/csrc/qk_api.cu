@@ -372,9 +372,10 @@ qk_status build_plan(qk_handle *h, const qk_contract *cs, int32_t n, const qk_gr
         const int ppt = choose_ppt(units, launch_units, h->sm_count,
                                    plain ? kPlainTilesPerWarp : h->tune_tpw[pr][cs[i].model][cs[i].scheme]);
         const bool tail = !plain && h->tune_tail[pr][cs[i].model][cs[i].scheme];
+        const int blk = plain ? kPathBlock : h->tune_block[pr][cs[i].model][cs[i].scheme];
         const int64_t warp_slots = static_cast<int64_t>(h->sm_count) *
-                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, lm, trk) *
-                                   (kPathBlock / 32);
+                                   price_tiles_max_blocks_per_sm(pr, cs[i].model, cs[i].scheme, lm, trk, blk) *
+                                   (blk / 32);
         const qk_greeks *g = plan.g_of(i);
         for (int role : roles_for(g, cs[i].T)) {
             const qk_contract b = bumped(plan.norm[i], g, role);
@@ -469,6 +470,20 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
             h->launches++;
         }
     } else {
+        // kinds on forked streams: every launch waits for the cursor reset and the start
+        // event; the handle's stream waits for all of them before the merge
+        int n_kinds = 0;
+        for (size_t i = 0; i < nt; ++i)
+            if (i == 0 || plan.tasks[i].precision != plan.tasks[i - 1].precision ||
+                plan.tasks[i].model != plan.tasks[i - 1].model || plan.tasks[i].scheme != plan.tasks[i - 1].scheme ||
+                plan.tasks[i].lane_mode != plan.tasks[i - 1].lane_mode || plan.tasks[i].track != plan.tasks[i - 1].track)
+                ++n_kinds;
+        const int n_streams = std::min(n_kinds, kKindStreams);
+        if (n_streams > 1) {
+            QK_CUDA_TRY(cudaEventRecordWithFlags(h->kind_fork, h->stream, 0));
+            for (int k = 0; k < n_streams; ++k) QK_CUDA_TRY(cudaStreamWaitEvent(h->kind_stream[k], h->kind_fork, 0));
+        }
+        int kind = 0;
         size_t b = 0;
         while (b < nt) {
             size_t e = b;
@@ -479,17 +494,27 @@ static qk_status enqueue_plan(qk_handle *h, const Plan &plan, bool capture) {
                 ++e;
             const int64_t slots_end = plan.tasks[e - 1].tile_begin + plan.tasks[e - 1].n_tiles;
             const int64_t slots = slots_end - tb.tile_begin;
-            const int per_sm = price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.lane_mode, tb.track);
+            const int blk = h->tune_block[tb.precision][tb.model][tb.scheme];
+            const int per_sm =
+                price_tiles_max_blocks_per_sm(tb.precision, tb.model, tb.scheme, tb.lane_mode, tb.track, blk);
             const int grid = static_cast<int>(std::min<int64_t>(slots, static_cast<int64_t>(h->sm_count) * per_sm));
             bool uniform_key = true;
             for (size_t i = b; i < e; ++i)
                 uniform_key &= plan.tasks[i].key0 == tb.key0 && plan.tasks[i].key1 == tb.key1;
             const uint64_t seed = static_cast<uint64_t>(tb.key0) | (static_cast<uint64_t>(tb.key1) << 32);
-            QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, h->stream, dt + b, dp + b,
+            cudaStream_t ks = n_streams > 1 ? h->kind_stream[kind % n_streams] : h->stream;
+            QK_CUDA_TRY(launch_price_tiles(tb.precision, tb.model, tb.scheme, grid, ks, dt + b, dp + b,
                                            static_cast<int32_t>(e - b), tb.tile_begin, slots_end, dc + b, dpart,
-                                           uniform_key, seed, tb.lane_mode, tb.track));
+                                           uniform_key, seed, tb.lane_mode, tb.track, blk));
             h->launches++;
+            ++kind;
             b = e;
+        }
+        if (n_streams > 1) {
+            for (int k = 0; k < n_streams; ++k) {
+                QK_CUDA_TRY(cudaEventRecordWithFlags(h->kind_join[k], h->kind_stream[k], 0));
+                QK_CUDA_TRY(cudaStreamWaitEvent(h->stream, h->kind_join[k], 0));
+            }
         }
     }
     QK_CUDA_TRY(cudaEventRecordWithFlags(h->ev_paths1, h->stream, ev_flags));
@@ -630,27 +655,30 @@ qk_status assemble_results(qk_handle *h, const Plan &plan, const Moments *task_m
     return QK_OK;
 }
 
-qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &out) {
+// Leg-0 payoffs (undiscounted, normalised units) of paths first .. first + count - 1.
+qk_status payoffs_range(qk_handle *h, const qk_contract &c, int64_t first, int64_t count, double *out) {
     qk_status s = validate_contract(c, nullptr);
     if (s != QK_OK) return s;
     if (c.antithetic) return fail(QK_ERR_UNSUPPORTED, "per-path payoffs of antithetic pairs are not dumped");
+    if (first < 0 || count < 1 || first + count > c.n_paths) return fail(QK_ERR_INVALID_ARG, "path range beyond n_paths");
     QK_CUDA_TRY(cudaSetDevice(h->device));
     double scale = 1.0;
     const qk_contract n = normalised(c, &scale);
     const TaskDev t = make_task(n, 1);
-    const size_t bytes = 256 + static_cast<size_t>(c.n_paths) * sizeof(double);
-    if ((s = h->d_trace.ensure(bytes)) != QK_OK) return s;
+    const size_t head = ((sizeof(TaskDev) + 255) / 256) * 256;
+    if ((s = h->d_trace.ensure(head + static_cast<size_t>(count) * sizeof(double))) != QK_OK) return s;
     TaskDev *dt = static_cast<TaskDev *>(h->d_trace.ptr);
-    double *dp = reinterpret_cast<double *>(static_cast<char *>(h->d_trace.ptr) + ((sizeof(TaskDev) + 255) / 256) * 256);
-    if ((s = h->d_trace.ensure(((sizeof(TaskDev) + 255) / 256) * 256 + c.n_paths * sizeof(double))) != QK_OK) return s;
-    dt = static_cast<TaskDev *>(h->d_trace.ptr);
-    dp = reinterpret_cast<double *>(static_cast<char *>(h->d_trace.ptr) + ((sizeof(TaskDev) + 255) / 256) * 256);
-    out.resize(static_cast<size_t>(c.n_paths));
+    double *dp = reinterpret_cast<double *>(static_cast<char *>(h->d_trace.ptr) + head);
     QK_CUDA_TRY(cudaMemcpyAsync(dt, &t, sizeof(TaskDev), cudaMemcpyHostToDevice, h->stream));
-    QK_CUDA_TRY(launch_payoff_paths(c.precision == QK_FP32 ? QK_FP32 : QK_FP64, h->stream, dt, c.n_paths, dp));
-    QK_CUDA_TRY(cudaMemcpyAsync(out.data(), dp, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QK_CUDA_TRY(launch_payoff_paths(c.precision == QK_FP32 ? QK_FP32 : QK_FP64, h->stream, dt, first, count, dp));
+    QK_CUDA_TRY(cudaMemcpyAsync(out, dp, static_cast<size_t>(count) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     QK_CUDA_TRY(cudaStreamSynchronize(h->stream));
     return QK_OK;
+}
+
+qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &out) {
+    out.resize(static_cast<size_t>(c.n_paths));
+    return payoffs_range(h, c, 0, c.n_paths, out.data());
 }
 
 qk_status finish_timing(qk_handle *h, double path_steps) {
@@ -690,6 +718,7 @@ qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const q
     }
     QK_CUDA_TRY(cudaEventRecord(h->ev_end, h->stream));
     QK_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (!h->plan.american.empty() && (s = lsm_check(h, h->plan)) != QK_OK) return s;
     if ((s = assemble_results(h, h->plan, static_cast<const Moments *>(h->h_moments.ptr), out)) != QK_OK) return s;
     if (!h->plan.american.empty()) assemble_lsm_results(h, h->plan, lsm_moments, out);
     double ps = h->plan.path_steps + h->plan.lsm_path_steps;
@@ -724,9 +753,14 @@ qk_status qk_create(int32_t device, qk_handle **out) {
     qk_handle *h = new qk_handle();
     h->device = device;
     h->sm_count = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&h->ev_start) != cudaSuccess || cudaEventCreate(&h->ev_paths0) != cudaSuccess ||
-        cudaEventCreate(&h->ev_paths1) != cudaSuccess || cudaEventCreate(&h->ev_end) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&h->ev_start) == cudaSuccess && cudaEventCreate(&h->ev_paths0) == cudaSuccess &&
+              cudaEventCreate(&h->ev_paths1) == cudaSuccess && cudaEventCreate(&h->ev_end) == cudaSuccess &&
+              cudaEventCreateWithFlags(&h->kind_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; ok && k < kKindStreams; ++k)
+        ok = cudaStreamCreateWithFlags(&h->kind_stream[k], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&h->kind_join[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         delete h;
         return fail(QK_ERR_CUDA, "stream/event creation failed");
     }
@@ -752,6 +786,11 @@ qk_status qk_destroy(qk_handle *h) {
     cudaEventDestroy(h->ev_start);
     cudaEventDestroy(h->ev_paths0);
     cudaEventDestroy(h->ev_paths1);
+    for (int k = 0; k < kKindStreams; ++k) {
+        cudaStreamDestroy(h->kind_stream[k]);
+        cudaEventDestroy(h->kind_join[k]);
+    }
+    cudaEventDestroy(h->kind_fork);
     cudaEventDestroy(h->ev_end);
     cudaStreamDestroy(h->stream);
     delete h;
@@ -853,6 +892,35 @@ qk_status qk_batch_fetch(qk_handle *h, qk_result *out, int32_t n) {
     qk_status s = assemble_results(h, h->plan, static_cast<const Moments *>(h->h_moments.ptr), out);
     if (s != QK_OK) return s;
     return finish_timing(h, h->plan.path_steps);
+}
+
+qk_status qk_payoffs_range(qk_handle *h, const qk_contract *c, int64_t first, int64_t count, double *payoffs) {
+    if (!h || !c || !payoffs) return fail(QK_ERR_INVALID_ARG, "NULL argument");
+    return payoffs_range(h, *c, first, count, payoffs);
+}
+
+qk_status qk_payoff_trace(const qk_payoff *leg, const double *S, int32_t n, double S0, int32_t precision,
+                          double *payoff) {
+    if (!leg || !S || !payoff || n < 1) return fail(QK_ERR_INVALID_ARG, "invalid payoff trace arguments");
+    if (leg->type < QK_EUROPEAN || leg->type > QK_BINARY_ASSET || (leg->right != QK_CALL && leg->right != QK_PUT))
+        return fail(QK_ERR_INVALID_ARG, "payoff type or right invalid (American legs have no path payoff)");
+    PayoffSpec ps{leg->type, leg->right, leg->strike, leg->barrier};
+    void *d = nullptr;
+    QK_CUDA_TRY(cudaMalloc(&d, (static_cast<size_t>(n) + 1) * sizeof(double)));
+    double *dS = static_cast<double *>(d);
+    double *dout = dS + n;
+    cudaError_t e = cudaMemcpy(dS, S, static_cast<size_t>(n) * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_payoff_trace(precision == QK_FP32 ? QK_FP32 : QK_FP64, 0, ps, dS, n, S0, dout);
+    if (e == cudaSuccess) e = cudaMemcpy(payoff, dout, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(QK_ERR_CUDA, std::string("qk_payoff_trace: ") + cudaGetErrorString(e));
+    return QK_OK;
+}
+
+qk_status qk_debug_lsm_withhold_block(qk_handle *h, int32_t block) {
+    if (!h) return fail(QK_ERR_INVALID_ARG, "NULL handle");
+    h->lsm_withhold_block = block < 0 ? -1 : block;
+    return QK_OK;
 }
 
 qk_status qk_step_trace(int32_t precision, const qk_contract *c, const double *z, const double *u, int32_t umax,

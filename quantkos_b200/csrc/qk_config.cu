@@ -307,16 +307,29 @@ int64_t stored_batch_paths(const qk_config &cfg, const qk_contract &c) {
 }
 
 template <class R>
+void write_paths_header(std::ofstream &f, int64_t n_paths, int n_steps, double dt, double scale) {
+    BinHeader<R> hd;
+    hd.total_n_sims = static_cast<int32_t>(n_paths);
+    hd.n_time_steps = n_steps;
+    hd.dt = static_cast<R>(dt);
+    hd.scale_factor = scale;
+    f.write(reinterpret_cast<const char *>(&hd), sizeof(hd));
+}
+
+// Rows of `count` paths x n_steps spot values in real units, stored normalised.
+template <class R>
+void write_paths_rows(std::ofstream &f, const double *S, int64_t count, int n_steps, double scale, std::vector<R> &row) {
+    row.resize(static_cast<size_t>(count) * n_steps);
+    for (size_t i = 0; i < row.size(); ++i) row[i] = static_cast<R>(S[i] / scale);  // payload holds normalised prices
+    f.write(reinterpret_cast<const char *>(row.data()), static_cast<std::streamsize>(row.size() * sizeof(R)));
+}
+
+template <class R>
 qk_status write_paths_file(qk_handle *h, const qk_contract &c, double dt, double scale, const std::string &path,
                            int64_t chunk) {
     std::ofstream f(path, std::ios::out | std::ios::binary);
     if (!f.is_open()) return fail(QK_ERR_INVALID_ARG, "[BinWriter Error] Failed to open binary output file: " + path);
-    BinHeader<R> hd;
-    hd.total_n_sims = static_cast<int32_t>(c.n_paths);
-    hd.n_time_steps = c.n_steps;
-    hd.dt = static_cast<R>(dt);
-    hd.scale_factor = scale;
-    f.write(reinterpret_cast<const char *>(&hd), sizeof(hd));
+    write_paths_header<R>(f, c.n_paths, c.n_steps, dt, scale);
     std::vector<double> S;
     std::vector<R> row;
     for (int64_t first = 0; first < c.n_paths; first += chunk) {
@@ -324,9 +337,7 @@ qk_status write_paths_file(qk_handle *h, const qk_contract &c, double dt, double
         S.resize(static_cast<size_t>(cnt) * c.n_steps);
         const qk_status st = qk_paths_dump(h, &c, first, cnt, S.data(), nullptr);
         if (st != QK_OK) return st;
-        row.resize(S.size());
-        for (size_t i = 0; i < S.size(); ++i) row[i] = static_cast<R>(S[i] / scale);  // payload holds normalised prices
-        f.write(reinterpret_cast<const char *>(row.data()), static_cast<std::streamsize>(row.size() * sizeof(R)));
+        write_paths_rows<R>(f, S.data(), cnt, c.n_steps, scale, row);
     }
     if (!f.good()) return fail(QK_ERR_INVALID_ARG, "[BinWriter Error] write failed: " + path);
     return QK_OK;
@@ -335,6 +346,25 @@ qk_status write_paths_file(qk_handle *h, const qk_contract &c, double dt, double
 }  // namespace
 
 extern "C" {
+
+qk_status qk_paths_write(const char *path, int32_t precision, int64_t n_paths, int32_t n_steps, double dt,
+                         double scale, const double *S) {
+    if (!path || !S || n_paths < 1 || n_steps < 1 || !(scale > 0.0))
+        return fail(QK_ERR_INVALID_ARG, "qk_paths_write: invalid arguments");
+    std::ofstream f(path, std::ios::out | std::ios::binary);
+    if (!f.is_open()) return fail(QK_ERR_INVALID_ARG, std::string("[BinWriter Error] Failed to open binary output file: ") + path);
+    if (precision == QK_FP32) {
+        std::vector<float> row;
+        write_paths_header<float>(f, n_paths, n_steps, dt, scale);
+        write_paths_rows<float>(f, S, n_paths, n_steps, scale, row);
+    } else {
+        std::vector<double> row;
+        write_paths_header<double>(f, n_paths, n_steps, dt, scale);
+        write_paths_rows<double>(f, S, n_paths, n_steps, scale, row);
+    }
+    if (!f.good()) return fail(QK_ERR_INVALID_ARG, std::string("[BinWriter Error] write failed: ") + path);
+    return QK_OK;
+}
 
 qk_status qk_config_default(qk_config *c) {
     if (!c) return fail(QK_ERR_INVALID_ARG, "NULL argument");

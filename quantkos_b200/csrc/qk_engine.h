@@ -29,7 +29,8 @@ struct HostArena {
 };
 
 struct LsmTaskInfo {
-    int contract, role, grid;
+    int contract, role, grid;  // grid: blocks whose moments the job wrote
+    int64_t moments_base;      // first of them in the per-block moments
     int64_t n_paths;
     double intrinsic0, eps;
 };
@@ -62,6 +63,9 @@ struct LsmArena {
 // American jobs of one call run on up to kLsmLanes streams at once, each stream with
 // its own working set, so that the fixed per-date cost of small jobs overlaps.
 constexpr int kLsmLanes = 4;
+// The persistent launches of the kernel kinds of one call run on up to kKindStreams
+// streams forked from the handle's stream, so that one kind's tail overlaps the next.
+constexpr int kKindStreams = 8;
 
 }  // namespace qk
 
@@ -73,6 +77,7 @@ using ShapeTable = std::array<std::array<std::array<int, 3>, 2>, 2>;
 constexpr ShapeTable kDefaultTilesPerWarp = {{{{{{24, 24, 24}}, {{24, 24, 24}}}}, {{{{48, 48, 48}}, {{48, 48, 48}}}}}};
 constexpr ShapeTable kDefaultGuidedTail = {{{{{{0, 0, 0}}, {{0, 0, 0}}}}, {{{{1, 1, 0}}, {{1, 1, 1}}}}}};
 constexpr ShapeTable kDefaultPathsPerLane = {{{{{{1, 1, 1}}, {{1, 1, 1}}}}, {{{{2, 2, 2}}, {{2, 2, 2}}}}}};
+constexpr ShapeTable kDefaultBlock = {{{{{{256, 256, 256}}, {{256, 256, 256}}}}, {{{{256, 256, 256}}, {{256, 256, 256}}}}}};
 
 struct qk_handle {
     int device = 0;
@@ -84,7 +89,13 @@ struct qk_handle {
     qk::DevArena d_lsm_moments;
     qk::LsmArena lsm[qk::kLsmLanes];
     qk::DevArena lsm_task, lsm_centre;    // descriptors and centring shifts of all jobs of a call
+    qk::DevArena lsm_sync;                // per job: the grid-wide synchronisation words of its backward launch
+    qk::HostArena h_lsm_sync;             // their copy after the call (error words)
+    int lsm_sync_stride = 0;
+    int lsm_withhold_block = -1;          // test hook (qk_debug_lsm_withhold_block)
     cudaStream_t lsm_stream[qk::kLsmLanes] = {};
+    cudaStream_t kind_stream[qk::kKindStreams] = {};
+    cudaEvent_t kind_fork = nullptr, kind_join[qk::kKindStreams] = {};
     cudaEvent_t lsm_fork = nullptr, lsm_join[qk::kLsmLanes] = {};
     qk::Plan plan;
     bool prepared = false;
@@ -95,6 +106,7 @@ struct qk_handle {
     ShapeTable tune_tpw = kDefaultTilesPerWarp;
     ShapeTable tune_tail = kDefaultGuidedTail;
     ShapeTable tune_lanes = kDefaultPathsPerLane;  // paths per lane: 1 or 2
+    ShapeTable tune_block = kDefaultBlock;         // threads per block of the pricing kernel
     qk_timing timing{};
     int64_t launches = 0;
     int64_t h2d_bytes = 0, d2h_bytes = 0;
@@ -119,11 +131,14 @@ qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const q
 
 // Every path's leg-0 payoff (undiscounted, normalised) of a contract, on the host.
 qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &out);
+qk_status payoffs_range(qk_handle *h, const qk_contract &c, int64_t first, int64_t count, double *out);
 
 // Longstaff-Schwartz for the American contracts of a plan (qk_lsm.cu).
 qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Moments> &moments);
 void assemble_lsm_results(qk_handle *h, const Plan &plan, const std::vector<Moments> &moments, qk_result *out);
 void lsm_release(qk_handle *h);
+// QK_ERR_TIMEOUT if a backward launch of the last call gave up a bounded wait.
+qk_status lsm_check(const qk_handle *h, const Plan &plan);
 qk_status lsm_events_ensure(qk_handle *h, size_t n);
 // Device time of the last call's LSM jobs: forward slab kernels and backward sweeps.
 void lsm_timing(qk_handle *h, double *paths_ms, double *sweep_ms);

@@ -424,15 +424,18 @@ __device__ __forceinline__ int find_task(const int64_t *__restrict__ prefix, int
 
 // LANE: kLaneOne (a lane simulates one path), kLanePair (an antithetic pair),
 // kLaneTwo (two independent paths 2u and 2u+1).
+// Blocks of 128, 256 or 512 threads (FP32; up to 256 in FP64): the register budget is
+// set for kPathMinBlocksFp32 resident 256-thread blocks per SM (64 registers a thread).
 template <class R, int MODEL, int SCHEME, bool UK, int LANE, bool TRK>
-__global__ void __launch_bounds__(kPathBlock, sizeof(R) == 4 ? kPathMinBlocksFp32 : 1)
+__global__ void __launch_bounds__(path_block_max<R>(),
+                                  sizeof(R) == 4 ? kPathMinBlocksFp32 * kPathBlock / path_block_max<R>() : 1)
     price_tiles_kernel(const TaskDev *__restrict__ tasks, const int64_t *__restrict__ prefix, int32_t n_tasks,
                        int64_t slot_begin, int64_t slot_end, unsigned long long *__restrict__ cursor,
                        Moments *__restrict__ partials, const PhiloxRoundKeys rk) {
     // Every warp is an independent worker: it pops a tile (kWarpTilePaths * ppt paths of one
     // task), keeps the tile's running moments per leg in its own shared-memory slots and
     // writes one record per leg.  No block-wide barrier anywhere.
-    __shared__ Moments s_acc[kPathBlock / 32][QK_MAX_PAYOFFS];
+    __shared__ Moments s_acc[path_block_max<R>() / 32][QK_MAX_PAYOFFS];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);  // OptionPricer.hpp:316
@@ -599,23 +602,37 @@ __device__ __forceinline__ void block_sum4(double &a, double &b, double &c, doub
     __syncthreads();
 }
 
+// Neumaier's compensated addition (Neumaier, ZAMM 54, 1974): s + c carries the sum
+// of the added values with the rounding error of every addition kept in c.
+__device__ __forceinline__ void neumaier_add(double &s, double &c, double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+}
+
 // Block-wide merge of rec[i * stride], i < count; the result is valid in thread 0.
+// Each thread sums its records' D and Q with compensation; the per-thread sums and
+// their compensations are reduced separately and added at the end.
 __device__ __forceinline__ Moments merge_range(const Moments *__restrict__ rec, int64_t count, int64_t stride,
                                                double (*red)[32]) {
     const double c = count > 0 ? rec[0].mean : 0.0;
-    double n = 0.0, D = 0.0, Q = 0.0, itm = 0.0;
+    double n = 0.0, D = 0.0, Q = 0.0, itm = 0.0, cD = 0.0, cQ = 0.0;
     for (int64_t i = threadIdx.x; i < count; i += blockDim.x) {
         const Moments m = rec[i * stride];
         const double d = m.mean - c;
         const double nd = m.n * d;
         n += m.n;
-        D += nd;
-        Q += fma(nd, d, m.m2);
+        neumaier_add(D, cD, nd);
+        neumaier_add(Q, cQ, fma(nd, d, m.m2));
         itm += m.itm;
     }
     block_sum4(n, D, Q, itm, red);
+    double z0 = 0.0, z1 = 0.0;
+    block_sum4(cD, cQ, z0, z1, red);
     Moments r{0.0, 0.0, 0.0, 0.0};
     if (n > 0.0) {
+        D += cD;
+        Q += cQ;
         r.n = n;
         r.mean = c + D / n;
         r.m2 = fmax(Q - D * (D / n), 0.0);
@@ -743,15 +760,41 @@ SlabKernel<R> slab_kernel_for(int model, int scheme) {
 // Per-path payoff of leg 0 (undiscounted, normalised units), for the payoff
 // distribution analysis (OptionPricer.hpp:340-360 sorts every path's payoff).
 template <class R>
-__global__ void __launch_bounds__(kPathBlock) payoff_paths_kernel(const TaskDev *__restrict__ task, int64_t count,
-                                                                 double *__restrict__ out) {
+__global__ void __launch_bounds__(kPathBlock) payoff_paths_kernel(const TaskDev *__restrict__ task, int64_t first,
+                                                                 int64_t count, double *__restrict__ out) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const TaskDev &t = *task;
     const StepConst<R> p = task_const<R>(t);
     PathState<R> st;
-    simulate_dispatch<R>(t, p, static_cast<uint32_t>(i), st, NoSink{});
+    simulate_dispatch<R>(t, p, static_cast<uint32_t>(first + i), st, NoSink{});
     out[i] = static_cast<double>(final_payoff<R>(t.pay[0], st.S, st.ssum, st.smax, st.smin, t.n_steps));
+}
+
+// Payoff of one leg on a fed spot sequence S_1..S_n (one thread): the path kernel's
+// tracking (running max / min, the Asian sum in blocks of kSumChunk steps in the working
+// precision folded into FP64) and final_payoff, on the given values instead of simulated
+// ones (PayoffTracker::track_current_price + evaluate_final_payoff, Payoff.hpp:84-243).
+template <class R>
+__global__ void payoff_trace_kernel(const PayoffSpec ps, const double *__restrict__ S, int n, double S0,
+                                    double *__restrict__ out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    PathState<R> st;
+    st.S = static_cast<R>(S0);
+    st.v = R(0);
+    st.ssum = 0.0;
+    st.smax = st.S;
+    st.smin = st.S;
+    for (int n0 = 0; n0 < n; n0 += kSumChunk) {
+        R blk = R(0);
+        const int n1 = min(n0 + kSumChunk, n);
+        for (int i = n0; i < n1; ++i) {
+            st.S = static_cast<R>(S[i]);
+            track(st, blk);
+        }
+        st.ssum += static_cast<double>(blk);
+    }
+    *out = static_cast<double>(final_payoff<R>(ps, st.S, st.ssum, st.smax, st.smin, n));
 }
 
 // Fed-draw trace of the step functions (one thread).
@@ -790,16 +833,22 @@ __global__ void step_trace_kernel(const TaskDev *__restrict__ task, const double
 cudaError_t launch_price_tiles(int precision, int model, int scheme, int grid, cudaStream_t s, const TaskDev *tasks,
                                const int64_t *prefix, int32_t n_tasks, int64_t slot_begin, int64_t slot_end,
                                unsigned long long *cursor, Moments *partials, bool uniform_key, uint64_t seed,
-                               int lane_mode, bool track) {
+                               int lane_mode, bool track, int block) {
+    if (!price_tiles_block_ok(precision, block)) return cudaErrorInvalidConfiguration;
     const PhiloxRoundKeys rk = philox_round_keys(static_cast<uint32_t>(seed & 0xFFFFFFFFull),
                                                  static_cast<uint32_t>(seed >> 32));
     if (precision == QK_FP32)
-        price_kernel_for<float>(model, scheme, uniform_key, lane_mode, track)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<float>(model, scheme, uniform_key, lane_mode, track)<<<grid, block, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     else
-        price_kernel_for<double>(model, scheme, uniform_key, lane_mode, track)<<<grid, kPathBlock, 0, s>>>(
+        price_kernel_for<double>(model, scheme, uniform_key, lane_mode, track)<<<grid, block, 0, s>>>(
             tasks, prefix, n_tasks, slot_begin, slot_end, cursor, partials, rk);
     return cudaGetLastError();
+}
+
+bool price_tiles_block_ok(int precision, int block) {
+    const int mx = precision == QK_FP32 ? path_block_max<float>() : path_block_max<double>();
+    return block >= 64 && block <= mx && block % 32 == 0;
 }
 
 cudaError_t launch_merge_tasks(int n_tasks, cudaStream_t s, const TaskDev *tasks, const Moments *partials,
@@ -854,12 +903,22 @@ cudaError_t launch_step_trace(int precision, cudaStream_t s, const TaskDev *task
     return cudaGetLastError();
 }
 
-cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t count, double *out) {
+cudaError_t launch_payoff_paths(int precision, cudaStream_t s, const TaskDev *task, int64_t first, int64_t count,
+                                double *out) {
     const int64_t blocks = (count + kPathBlock - 1) / kPathBlock;
     if (precision == QK_FP32)
-        payoff_paths_kernel<float><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(task, count, out);
+        payoff_paths_kernel<float><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(task, first, count, out);
     else
-        payoff_paths_kernel<double><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(task, count, out);
+        payoff_paths_kernel<double><<<static_cast<unsigned>(blocks), kPathBlock, 0, s>>>(task, first, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_payoff_trace(int precision, cudaStream_t s, const PayoffSpec &ps, const double *S, int n, double S0,
+                                double *out) {
+    if (precision == QK_FP32)
+        payoff_trace_kernel<float><<<1, 1, 0, s>>>(ps, S, n, S0, out);
+    else
+        payoff_trace_kernel<double><<<1, 1, 0, s>>>(ps, S, n, S0, out);
     return cudaGetLastError();
 }
 
@@ -906,14 +965,14 @@ cudaError_t preload_noalloc_kernels() {
     return e;
 }
 
-int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode, bool track) {
+int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode, bool track, int block) {
     int nb = 0;
     if (precision == QK_FP32)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &nb, price_kernel_for<float>(model, scheme, true, lane_mode, track), kPathBlock, 0);
+            &nb, price_kernel_for<float>(model, scheme, true, lane_mode, track), block, 0);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &nb, price_kernel_for<double>(model, scheme, true, lane_mode, track), kPathBlock, 0);
+            &nb, price_kernel_for<double>(model, scheme, true, lane_mode, track), block, 0);
     return nb > 0 ? nb : 1;
 }
 

@@ -1,15 +1,21 @@
 // Continuous-batching request loop.
 //
-// Requests are queued by qk_serve_submit (any thread).  Lanes — host threads,
-// each with its own handle and CUDA stream on the same device — take whatever
-// has arrived, in arrival order, as long as the HBM the requests need fits in
-// what the budget has free, and price it as one batch (one persistent launch
-// plus the LSM sweeps of its American contracts).  While one lane's batch is on
-// the GPU, the next lane admits the requests that arrived meanwhile, so their
-// work overlaps on the device; memory is returned to the budget as each batch
-// completes.  A request larger than the whole budget is rejected
-// (QK_ERR_CAPACITY).  The reference has no serving layer (one contract per
-// process run, include/core/engine/Distpatcher.hpp:78-83).
+// Requests are queued by qk_serve_submit (any thread).  Lanes — host threads, each
+// with its own handle, CUDA stream and grow-only device arenas on the same device —
+// take the requests that have arrived, in arrival order, as one wave: a wave is
+// closed when its estimated GPU time reaches the larger of the wave budget (a few
+// milliseconds) and the lane's share of the backlog, when it reaches max_batch
+// requests, or when the HBM its requests need (LSM slabs and tile records) would
+// exceed what the budget has free.  Short queues thus give short waves (latency),
+// long queues long ones (throughput).  A wave is planned,
+// uploaded (each request's descriptors are copied to the device once, when its wave
+// starts) and priced as one persistent launch per kernel kind plus the LSM jobs of
+// its American contracts.  With several lanes, several waves are on the GPU at once:
+// a request that arrives while others are being priced is admitted into the next
+// wave as soon as a lane is free, its kernels overlap the waves already running, and
+// memory returns to the budget as each wave completes.  A request larger than the
+// whole budget is rejected (QK_ERR_CAPACITY).  The reference has no serving layer
+// (one contract per process run, include/core/engine/Distpatcher.hpp:78-83).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +42,7 @@ struct Request {
     qk_contract c;
     qk_greeks g;
     size_t bytes;
+    double est_us;
     Clock::time_point t_submit;
 };
 
@@ -45,13 +52,19 @@ struct Finished {
     double latency_ms;
 };
 
+bool is_american(const qk_contract &c) {
+    for (int k = 0; k < c.n_payoffs; ++k)
+        if (c.payoffs[k].type == QK_AMERICAN) return true;
+    return false;
+}
+
 // HBM a request holds while it is being priced: LSM slabs and cash flows for
 // American contracts, per-tile moment records and descriptors otherwise.
 size_t footprint(const qk_contract &c, const qk_greeks &g) {
     const size_t roles = qk::roles_for(g.mask ? &g : nullptr, c.T).size();
     const size_t esz = c.precision == QK_FP32 ? 4 : 8;
     size_t bytes = roles * (sizeof(qk::TaskDev) + 64);
-    if (c.payoffs[0].type == QK_AMERICAN) {
+    if (is_american(c)) {
         const size_t D = c.lsm_dates > 0 ? c.lsm_dates : c.n_steps;
         const size_t ld = (static_cast<size_t>(c.n_paths) + 3) / 4 * 4;
         const size_t slabs = c.lsm_basis == QK_LSM_POLY_SV ? 2 : 1;
@@ -65,12 +78,34 @@ size_t footprint(const qk_contract &c, const qk_greeks &g) {
     return bytes;
 }
 
+// Estimated GPU time of a request in microseconds: path-steps of all its pricing tasks
+// at the measured rate of the FP32 Heston-Euler kernel (5.4e11 path-steps/s), weighted
+// by the kind's relative cost (QE, jumps, FP64), plus for an American contract its
+// backward sweep (16 bytes per path and date at 3e12 B/s, and a fixed 10 us per date).
+double estimate_us(const qk_contract &c, const qk_greeks &g) {
+    const double roles = static_cast<double>(qk::roles_for(g.mask ? &g : nullptr, c.T).size());
+    double f = 1.0;
+    if (c.scheme == QK_ANDERSEN_QE) f *= 1.7;
+    if (c.scheme == QK_IMPLICIT_MILSTEIN) f *= 1.06;
+    if (c.model == QK_BATES) f *= 1.2;
+    if (c.precision == QK_FP64) f *= 6.0;
+    double us = roles * static_cast<double>(c.n_paths) * c.n_steps * f / 5.4e5;
+    if (is_american(c)) {
+        const double D = c.lsm_dates > 0 ? c.lsm_dates : c.n_steps;
+        us += roles * (16.0 * static_cast<double>(c.n_paths) * D / 3e6 + 10.0 * D);
+    }
+    return us;
+}
+
 }  // namespace
 
 struct qk_server {
     int device = 0;
     size_t budget = 0, in_use = 0;
     int max_batch = 256;
+    double wave_us = 8000.0;  // GPU-time budget of one wave (the least a wave is allowed to hold)
+    double queued_us = 0.0;   // estimated GPU time of the requests waiting for admission
+    int n_lanes = 1;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request> queue;
@@ -99,12 +134,20 @@ static void lane_loop(qk_server *s, qk_handle *h) {
             std::unique_lock<std::mutex> lk(s->mu);
             for (;;) {
                 if (s->stop && s->queue.empty()) return;
+                // wave size: the budget, or this lane's share of the backlog when that is larger
+                // (small waves while the queue is short, large ones under load)
+                const double cap = std::max(s->wave_us, s->queued_us / s->n_lanes);
+                double est = 0.0;
                 while (!s->queue.empty() && static_cast<int>(batch.size()) < s->max_batch &&
-                       s->in_use + bytes + s->queue.front().bytes <= s->budget) {
+                       s->in_use + bytes + s->queue.front().bytes <= s->budget &&
+                       (batch.empty() || est + s->queue.front().est_us <= cap)) {
                     bytes += s->queue.front().bytes;
+                    est += s->queue.front().est_us;
+                    s->queued_us -= s->queue.front().est_us;
                     batch.push_back(s->queue.front());
                     s->queue.pop_front();
                 }
+                if (s->queue.empty()) s->queued_us = 0.0;  // no drift from rounding
                 if (!batch.empty()) break;
                 s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
             }
@@ -146,8 +189,20 @@ static void lane_loop(qk_server *s, qk_handle *h) {
 extern "C" {
 
 qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch, qk_server **out) {
-    if (!h || !out) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    qk_serve_options o;
+    std::memset(&o, 0, sizeof(o));
+    o.hbm_budget_mib = hbm_budget_mib;
+    o.max_batch = max_batch;
+    return qk_serve_start_ex(h, &o, out);
+}
+
+qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server **out) {
+    if (!h || !opt || !out) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
     *out = nullptr;
+    if (opt->lanes < 0 || opt->lanes > 16) return qk::fail(QK_ERR_INVALID_ARG, "lanes must be in [0, 16] (0 = 4)");
+    if (opt->wave_ms < 0.0) return qk::fail(QK_ERR_INVALID_ARG, "wave_ms must be >= 0 (0 = 8 ms)");
+    const int64_t hbm_budget_mib = opt->hbm_budget_mib;
+    const int32_t max_batch = opt->max_batch;
     if (cudaSetDevice(h->device) != cudaSuccess) return qk::fail(QK_ERR_CUDA, "cudaSetDevice failed");
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return qk::fail(QK_ERR_CUDA, "cudaMemGetInfo failed");
@@ -155,8 +210,10 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
     s->device = h->device;
     s->budget = hbm_budget_mib > 0 ? static_cast<size_t>(hbm_budget_mib) << 20 : static_cast<size_t>(free_b * 0.8);
     s->max_batch = max_batch > 0 ? max_batch : 256;
-    constexpr int kLanes = 2;
-    for (int i = 0; i < kLanes; ++i) {
+    s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 8000.0;
+    const int lanes = opt->lanes > 0 ? opt->lanes : 4;
+    s->n_lanes = lanes;
+    for (int i = 0; i < lanes; ++i) {
         qk_handle *lh = nullptr;
         const qk_status st = qk_create(h->device, &lh);
         if (st != QK_OK) {
@@ -169,6 +226,7 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
         lh->tune_tpw = h->tune_tpw;
         lh->tune_tail = h->tune_tail;
         lh->tune_lanes = h->tune_lanes;
+        lh->tune_block = h->tune_block;
         s->handles.push_back(lh);
     }
     for (qk_handle *lh : s->handles) s->lanes.emplace_back(lane_loop, s, lh);
@@ -185,6 +243,7 @@ qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g
     if (g) r.g = *g;
     else std::memset(&r.g, 0, sizeof(r.g));
     r.bytes = footprint(r.c, r.g);
+    r.est_us = estimate_us(r.c, r.g);
     r.t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return qk::fail(QK_ERR_STATE, "server stopped");
@@ -199,6 +258,7 @@ qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g
     }
     r.ticket = s->next_ticket++;
     *ticket = r.ticket;
+    s->queued_us += r.est_us;
     s->queue.push_back(r);
     s->cv_work.notify_one();
     return QK_OK;
@@ -230,6 +290,7 @@ qk_status qk_serve_cancel(qk_server *s, int64_t ticket, int32_t *cancelled) {
         if (ticket <= 0 || ticket >= s->next_ticket) return qk::fail(QK_ERR_STATE, "unknown ticket");
         auto it = std::find_if(s->queue.begin(), s->queue.end(), [&](const Request &r) { return r.ticket == ticket; });
         if (it == s->queue.end()) return QK_OK;  // admitted already (or finished): it completes
+        s->queued_us = std::max(0.0, s->queued_us - it->est_us);
         s->queue.erase(it);
         Finished f;
         std::memset(&f.r, 0, sizeof(f.r));

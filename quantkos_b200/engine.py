@@ -107,7 +107,7 @@ class Handle:
               "qk_autotune")
         return [{"precision": rep.precision[k], "model": rep.model[k], "scheme": rep.scheme[k],
                  "tiles_per_warp": rep.tiles_per_warp[k], "guided_tail": rep.guided_tail[k],
-                 "paths_per_lane": rep.paths_per_lane[k],
+                 "paths_per_lane": rep.paths_per_lane[k], "block_size": rep.block_size[k],
                  "best_ms": rep.best_ms[k], "default_ms": rep.default_ms[k]} for k in range(rep.n_kinds)]
 
     def tune_reset(self) -> None:
@@ -115,9 +115,11 @@ class Handle:
         check(L.lib().qk_tune_reset(self.ptr), "qk_tune_reset")
 
     def tune_set(self, precision: int, model: int, scheme: int, tiles_per_warp: int, guided_tail: bool,
-                 paths_per_lane: int = 1) -> None:
+                 paths_per_lane: int = 1, block_size: int | None = None) -> None:
         check(L.lib().qk_tune_set(self.ptr, precision, model, scheme, tiles_per_warp, int(guided_tail),
                                   paths_per_lane), "qk_tune_set")
+        if block_size is not None:
+            check(L.lib().qk_tune_set_block(self.ptr, precision, model, scheme, block_size), "qk_tune_set_block")
 
 
 _default: Handle | None = None
@@ -358,10 +360,14 @@ class MCDispatcher:
 class Server:
     """Continuous-batching request loop (qk_serve_*)."""
 
-    def __init__(self, handle: Handle | None = None, hbm_budget_mib: int = 0, max_batch: int = 256):
+    def __init__(self, handle: Handle | None = None, hbm_budget_mib: int = 0, max_batch: int = 256, lanes: int = 0,
+                 wave_ms: float = 0.0):
+        """lanes: host threads whose waves run on the GPU at once (0 = 4); wave_ms: estimated GPU time at
+        which a lane closes a wave (0 = 8 ms)."""
         self.handle = handle or default_handle()
         self._s = C.c_void_p()
-        check(L.lib().qk_serve_start(self.handle.ptr, hbm_budget_mib, max_batch, C.byref(self._s)), "qk_serve_start")
+        opt = L.ServeOptions(hbm_budget_mib, max_batch, lanes, wave_ms)
+        check(L.lib().qk_serve_start_ex(self.handle.ptr, C.byref(opt), C.byref(self._s)), "qk_serve_start_ex")
 
     def submit(self, contract: L.Contract, greeks: L.Greeks | None = None) -> int:
         t = C.c_int64()

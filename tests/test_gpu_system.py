@@ -310,7 +310,7 @@ def test_server_cancels_waiting_requests(qk, handle):
     from quantkos_b200 import workloads as W
     long_job = W.bates_qe_five_payoffs(n_paths=16_777_216)  # keeps both lanes busy for tens of ms
     small = qk.make_contract(n_paths=10_000, n_steps=10)
-    with qk.Server(handle, 0, 1) as srv:  # one request per batch
+    with qk.Server(handle, 0, 1, lanes=2) as srv:  # one request per wave, two lanes
         t_busy = [srv.submit(long_job) for _ in range(2)]
         t_keep = srv.submit(small)
         t_drop = srv.submit(small)
