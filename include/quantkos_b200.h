@@ -254,15 +254,6 @@ qk_status qk_tune_set(qk_handle *h, int32_t precision, int32_t model, int32_t sc
  * stream); the call returns after its work has finished. */
 qk_status qk_price_noalloc(const qk_contract *c, void *stream, qk_result *out);
 
-/* ---------------------------------------------------------------- failure-path testing
- * qk_debug_lsm_withhold_block — no counterpart in the reference.  The backward
- * induction of an American job runs as one launch whose blocks wait, with a bound of
- * about a second, for each exercise date's coefficients.  With block >= 0, block
- * `block` of every later backward launch on h leaves before its first arrival, so
- * the other blocks' waits run out: the pricing call returns QK_ERR_TIMEOUT and the
- * device stays usable.  block < 0 restores normal operation.  For tests only. */
-qk_status qk_debug_lsm_withhold_block(qk_handle *h, int32_t block);
-
 /* ---------------------------------------------------------------- parity harness
  * qk_step_trace — SDEScheme<M,S>::evolve_step with fed draws
  * (include/core/schemes/markovian/MSchemes.hpp:133-156, 229-253, 363-442, 493-526),

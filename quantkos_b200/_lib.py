@@ -146,7 +146,6 @@ SIGNATURES = {
     "qk_batch_run": (C.c_int, [_VP]),
     "qk_batch_fetch": (C.c_int, [_VP, _P(Result), C.c_int32]),
     "qk_price_noalloc": (C.c_int, [_P(Contract), _VP, _P(Result)]),
-    "qk_debug_lsm_withhold_block": (C.c_int, [_VP, C.c_int32]),
     "qk_payoff_trace": (C.c_int, [_P(Payoff), _P(C.c_double), C.c_int32, C.c_double, C.c_int32, _P(C.c_double)]),
     "qk_payoffs_range": (C.c_int, [_VP, _P(Contract), C.c_int64, C.c_int64, _P(C.c_double)]),
     "qk_lsm_date": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64, _P(C.c_double),

@@ -718,7 +718,6 @@ qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const q
     }
     QK_CUDA_TRY(cudaEventRecord(h->ev_end, h->stream));
     QK_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    if (!h->plan.american.empty() && (s = lsm_check(h, h->plan)) != QK_OK) return s;
     if ((s = assemble_results(h, h->plan, static_cast<const Moments *>(h->h_moments.ptr), out)) != QK_OK) return s;
     if (!h->plan.american.empty()) assemble_lsm_results(h, h->plan, lsm_moments, out);
     double ps = h->plan.path_steps + h->plan.lsm_path_steps;
@@ -914,12 +913,6 @@ qk_status qk_payoff_trace(const qk_payoff *leg, const double *S, int32_t n, doub
     if (e == cudaSuccess) e = cudaMemcpy(payoff, dout, sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) return fail(QK_ERR_CUDA, std::string("qk_payoff_trace: ") + cudaGetErrorString(e));
-    return QK_OK;
-}
-
-qk_status qk_debug_lsm_withhold_block(qk_handle *h, int32_t block) {
-    if (!h) return fail(QK_ERR_INVALID_ARG, "NULL handle");
-    h->lsm_withhold_block = block < 0 ? -1 : block;
     return QK_OK;
 }
 

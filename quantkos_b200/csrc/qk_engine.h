@@ -89,10 +89,6 @@ struct qk_handle {
     qk::DevArena d_lsm_moments;
     qk::LsmArena lsm[qk::kLsmLanes];
     qk::DevArena lsm_task, lsm_centre;    // descriptors and centring shifts of all jobs of a call
-    qk::DevArena lsm_sync;                // per job: the grid-wide synchronisation words of its backward launch
-    qk::HostArena h_lsm_sync;             // their copy after the call (error words)
-    int lsm_sync_stride = 0;
-    int lsm_withhold_block = -1;          // test hook (qk_debug_lsm_withhold_block)
     cudaStream_t lsm_stream[qk::kLsmLanes] = {};
     cudaStream_t kind_stream[qk::kKindStreams] = {};
     cudaEvent_t kind_fork = nullptr, kind_join[qk::kKindStreams] = {};
@@ -137,8 +133,6 @@ qk_status payoffs_range(qk_handle *h, const qk_contract &c, int64_t first, int64
 qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Moments> &moments);
 void assemble_lsm_results(qk_handle *h, const Plan &plan, const std::vector<Moments> &moments, qk_result *out);
 void lsm_release(qk_handle *h);
-// QK_ERR_TIMEOUT if a backward launch of the last call gave up a bounded wait.
-qk_status lsm_check(const qk_handle *h, const Plan &plan);
 qk_status lsm_events_ensure(qk_handle *h, size_t n);
 // Device time of the last call's LSM jobs: forward slab kernels and backward sweeps.
 void lsm_timing(qk_handle *h, double *paths_ms, double *sweep_ms);

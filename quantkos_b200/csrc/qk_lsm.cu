@@ -838,363 +838,6 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_final_kernel(LsmArgs a, const R
     }
 }
 
-// ---------------------------------------------------------------- persistent backward induction
-// The whole backward induction of one job in one cooperative launch (every block
-// resident).  Block b owns chunks b + k * gridDim.x on every date, so the cash flows
-// of its paths are read and written by this block alone from date to date.  Pass p
-// applies the exercise decision of date du = D-1-p (the maturity payoff when p = 0)
-// and accumulates the regression sums of date du-1, exactly as one launch of
-// lsm_sweep_kernel; the final pass (du = 0) applies date 0's decision, discounts to
-// t = 0 and writes per-block moments.  Between passes, a deterministic two-level
-// reduction publishes the next date's coefficients: a block adds its sums to its
-// group of kLsmGroup blocks, the last block of a group to arrive reduces the group
-// in block order, and the last group reducer reduces the group sums in group order,
-// solves in FP64 and publishes the coefficients with a release store of the pass
-// count (`epoch`).  The first stages of the next pass (slab rows and this block's
-// own cash flows, which do not depend on the coefficients) are queued before a block
-// waits for that epoch.
-//
-// Every wait is bounded: a block that has not seen the epoch after about a second
-// (QK_LSM_SPIN_LIMIT polls of at least 256 ns) sets the error word, waits for its own
-// copies in flight and returns; so do blocks that find the error word set.  The host
-// reads the error word and reports QK_ERR_TIMEOUT; the context stays usable.
-constexpr int kLsmGroup = 16;  // blocks per first-level reduction group
-#ifndef QK_LSM_SPIN_LIMIT
-#define QK_LSM_SPIN_LIMIT (1u << 22)
-#endif
-// Synchronisation words of one launch (zeroed by the host before it): [0] epoch =
-// passes whose coefficients are published, [1] error, [2] group reducers arrived
-// (counted over all passes), [3 + g] blocks of group g arrived (counted over all passes).
-constexpr int kLsmSyncHeader = 3;
-__host__ __device__ constexpr int lsm_sync_words(int grid) { return kLsmSyncHeader + (grid + kLsmGroup - 1) / kLsmGroup; }
-
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Thread 0: wait (bounded) until `target` passes are published; false if the wait
-// gave up or another block reported an error.
-__device__ __forceinline__ bool lsm_wait_epoch(unsigned *sync, unsigned target) {
-    for (unsigned i = 0; i < QK_LSM_SPIN_LIMIT; ++i) {
-        if (ld_acquire_u32(sync) >= target) return true;
-        if (ld_acquire_u32(sync + 1) != 0u) return false;
-        __nanosleep(256);
-    }
-    atomicExch(sync + 1, 1u);
-    return false;
-}
-
-template <class R, int BASIS>
-__global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS)
-    lsm_backward_kernel(LsmArgs a, const R *__restrict__ slab_S, const R *__restrict__ slab_v, R *__restrict__ cf,
-                        double *__restrict__ coeffs, int *__restrict__ flags, const double *__restrict__ centre,
-                        double *__restrict__ block_sums, double *__restrict__ group_sums, unsigned *__restrict__ sync,
-                        Moments *__restrict__ block_moments, int withhold_block) {
-    constexpr int NB = BasisTraits<BASIS>::NB;
-    constexpr int NSUM = Sums<NB>::NSUM;
-    constexpr int NACC = AccTraits<BASIS>::N;
-    constexpr bool use_v = BASIS == QK_LSM_POLY_SV;
-    constexpr bool kF32 = lsm_f32_poly<R, BASIS>();
-    constexpr int ST = lsm_stages<R>();
-    constexpr int kPer16 = 16 / static_cast<int>(sizeof(R));
-    using L = StageLayout<BASIS>;
-    extern __shared__ __align__(16) unsigned char lsm_smem[];
-    R *stage = reinterpret_cast<R *>(lsm_smem);
-    __shared__ double cu[kMaxCoef];
-    __shared__ float cuf[kMaxCoef];
-    __shared__ double s_red[kLsmBlock / 32][NACC];
-    __shared__ double s_tot[NACC];
-    __shared__ Moments s_mom[kLsmBlock / 32];
-    __shared__ int s_ok, s_group_last, s_all_last;
-
-    const int G = static_cast<int>(gridDim.x);
-    const int b = static_cast<int>(blockIdx.x);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int64_t n_chunks = (a.ld + kLsmChunk - 1) / kLsmChunk;
-    const int D = a.n_dates;
-
-    // Queue the copies of one chunk into stage st: spot (and variance) of the update
-    // date du (read for the last time: L2 evict-first), of the Gram date dg (read again
-    // by the next pass: evict-last; dg < 0 = none) and, unless init, the block's own cash
-    // flows.  Rows hold ld elements, ld a multiple of 4: no 16-byte group straddles a row.
-    auto issue = [&](int du, int dg, bool init, int64_t chunk, int st) {
-        R *base = stage + static_cast<size_t>(st) * L::kArrays * kLsmChunk;
-        const int64_t p0 = chunk * kLsmChunk;
-        const uint64_t pol_first = l2_policy_evict_first();
-        const uint64_t pol_last = l2_policy_evict_last();
-        for (int e = tid * kPer16; e < kLsmChunk; e += kLsmBlock * kPer16) {
-            const int64_t i = p0 + e;
-            if (i >= a.ld) break;
-            cp_async16(base + L::kSu * kLsmChunk + e, slab_S + static_cast<int64_t>(du) * a.ld + i, pol_first);
-            if (dg >= 0) cp_async16(base + L::kSg * kLsmChunk + e, slab_S + static_cast<int64_t>(dg) * a.ld + i, pol_last);
-            if constexpr (use_v) {
-                cp_async16(base + L::kVu * kLsmChunk + e, slab_v + static_cast<int64_t>(du) * a.ld + i, pol_first);
-                if (dg >= 0)
-                    cp_async16(base + L::kVg * kLsmChunk + e, slab_v + static_cast<int64_t>(dg) * a.ld + i, pol_last);
-            }
-            if (!init) cp_async16(base + L::kCf * kLsmChunk + e, cf + i, pol_last);
-        }
-    };
-    // Start of pass p: queue the first ST-1 chunks (groups 0 .. ST-2; loop iteration k
-    // then commits chunk k + ST - 1, possibly an empty group, so chunk k has landed once
-    // at most ST - 2 groups are pending), then wait for date du's coefficients (published
-    // by pass p - 1) and load them into shared memory.  False: the wait gave up.
-    auto begin_pass = [&](int p, int du, int dg, bool init) -> bool {
-        for (int s = 0; s < ST - 1; ++s) {
-            const int64_t c = b + static_cast<int64_t>(s) * G;
-            if (c < n_chunks) issue(du, dg, init, c, s);
-            cp_async_commit();
-        }
-        if (!init) {
-            if (tid == 0) s_ok = lsm_wait_epoch(sync, static_cast<unsigned>(p)) ? 1 : 0;
-            __syncthreads();
-            if (!s_ok) {
-                cp_async_wait_all();  // no copy of this block lands after it has left
-                return false;
-            }
-        }
-        if (tid < NB) {
-            const double c = init ? 0.0 : __ldcg(coeffs + du * kMaxCoef + tid);
-            cu[tid] = c;
-            cuf[tid] = static_cast<float>(c);
-        }
-        __syncthreads();  // coefficients visible
-        return true;
-    };
-
-    // ---- passes with a Gram date: decision at du = D-1-p, sums of dg = du - 1
-    for (int p = 0; p + 1 < D; ++p) {
-        const int du = D - 1 - p, dg = du - 1;
-        const bool init = p == 0;
-        if (!begin_pass(p, du, dg, init)) return;
-        const R K = static_cast<R>(a.K);
-        const double inv_K = 1.0 / a.K;
-        const float inv_Kf = static_cast<float>(inv_K);
-        const R disc = static_cast<R>(a.disc);
-        const double cxu = init ? 0.0 : centre[2 * du], cvu = init ? 0.0 : centre[2 * du + 1];
-        const double cxg = centre[2 * dg], cvg = centre[2 * dg + 1];
-        const float cxuf = static_cast<float>(cxu), cvuf = static_cast<float>(cvu);
-        const float cxgf = static_cast<float>(cxg), cvgf = static_cast<float>(cvg);
-        float2 cc[kF32 ? 6 : 1];
-        if constexpr (kF32) {
-#pragma unroll
-            for (int i = 0; i < 6; ++i) cc[i] = make_float2(cuf[i], cuf[i]);
-        }
-        double acc[NACC];
-#pragma unroll
-        for (int j = 0; j < NACC; ++j) acc[j] = 0.0;
-        float2 acc2[kF32 ? NACC : 1];
-#pragma unroll
-        for (int j = 0; j < (kF32 ? NACC : 1); ++j) acc2[j] = make_float2(0.0f, 0.0f);
-        auto flush = [&]() {
-            if constexpr (kF32) {
-#pragma unroll
-                for (int j = 0; j < NACC; ++j) {
-                    acc[j] += static_cast<double>(acc2[j].x + acc2[j].y);
-                    acc2[j] = make_float2(0.0f, 0.0f);
-                }
-            }
-        };
-        int64_t chunk = b;
-        for (int k = 0; chunk < n_chunks; ++k, chunk += G) {
-            cp_async_wait_pending<ST - 2>();
-            __syncthreads();  // every thread's copies of `chunk` landed; chunk k - 1's stage is free
-            const int64_t ahead = chunk + static_cast<int64_t>(ST - 1) * G;
-            if (ahead < n_chunks) issue(du, dg, init, ahead, (k + ST - 1) % ST);
-            cp_async_commit();
-            const R *base = stage + static_cast<size_t>(k % ST) * L::kArrays * kLsmChunk;
-            const int j0 = 4 * tid;
-            const int64_t i0 = chunk * kLsmChunk + j0;
-            if constexpr (kF32) {
-                if (i0 < a.N) {
-                    float S4[4], c4[4], v4[4];
-                    load4(base + L::kSu * kLsmChunk + j0, S4);
-                    if (!init) load4(base + L::kCf * kLsmChunk + j0, c4);
-                    load4(base + L::kVu * kLsmChunk + j0, v4);
-                    if (init) {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) c4[q] = lsm_intrinsic<float>(a.right, S4[q], K);
-                    } else {
-#pragma unroll
-                        for (int h = 0; h < 4; h += 2) {
-                            const float2 x = __ffma2_rn(make_float2(S4[h], S4[h + 1]), make_float2(inv_Kf, inv_Kf),
-                                                        make_float2(-cxuf, -cxuf));
-                            const float2 w = __fadd2_rn(make_float2(v4[h], v4[h + 1]), make_float2(-cvuf, -cvuf));
-                            const float2 hold = continuation_f32x2(cc, x, w);
-                            const float iv0 = lsm_intrinsic<float>(a.right, S4[h], K);
-                            const float iv1 = lsm_intrinsic<float>(a.right, S4[h + 1], K);
-                            c4[h] = (iv0 > 0.0f && iv0 > hold.x) ? iv0 : c4[h] * disc;
-                            c4[h + 1] = (iv1 > 0.0f && iv1 > hold.y) ? iv1 : c4[h + 1] * disc;
-                        }
-                    }
-                    store4(cf + i0, c4);  // i0 + 3 < ld: rows are padded to a multiple of 4
-                    float Sg4[4], vg4[4], x[4], w[4], y[4], one[4];
-                    load4(base + L::kSg * kLsmChunk + j0, Sg4);
-                    load4(base + L::kVg * kLsmChunk + j0, vg4);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const bool itm = i0 + q < a.N && lsm_intrinsic<float>(a.right, Sg4[q], K) > 0.0f;
-                        x[q] = itm ? fmaf(Sg4[q], inv_Kf, -cxgf) : 0.0f;
-                        w[q] = itm ? vg4[q] - cvgf : 0.0f;
-                        y[q] = itm ? c4[q] * disc : 0.0f;
-                        one[q] = itm ? 1.0f : 0.0f;
-                    }
-                    accumulate_f32x2(acc2, make_float2(x[0], x[1]), make_float2(w[0], w[1]), make_float2(y[0], y[1]),
-                                     make_float2(one[0], one[1]));
-                    accumulate_f32x2(acc2, make_float2(x[2], x[3]), make_float2(w[2], w[3]), make_float2(y[2], y[3]),
-                                     make_float2(one[2], one[3]));
-                }
-                if ((k & (kF32Flush - 1)) == kF32Flush - 1) flush();
-            } else {
-                if (i0 < a.N) {
-                    R S4[4], c4[4], v4[4] = {R(0), R(0), R(0), R(0)};
-                    load4(base + L::kSu * kLsmChunk + j0, S4);
-                    if (!init) load4(base + L::kCf * kLsmChunk + j0, c4);
-                    if (use_v) load4(base + L::kVu * kLsmChunk + j0, v4);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const R iv = lsm_intrinsic<R>(a.right, S4[q], K);
-                        if (init) {
-                            c4[q] = iv;
-                        } else {
-                            R c = c4[q] * disc;
-                            if (iv > R(0)) {
-                                const double hold = continuation<R, BASIS>(cu, S4[q], v4[q], K, inv_K, cxu, cvu);
-                                if (static_cast<double>(iv) > hold) c = iv;
-                            }
-                            c4[q] = c;
-                        }
-                    }
-                    store4(cf + i0, c4);
-                    R Sg4[4], vg4[4] = {R(0), R(0), R(0), R(0)};
-                    load4(base + L::kSg * kLsmChunk + j0, Sg4);
-                    if (use_v) load4(base + L::kVg * kLsmChunk + j0, vg4);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        if (i0 + q < a.N && lsm_intrinsic<R>(a.right, Sg4[q], K) > R(0))
-                            accumulate<R, BASIS>(acc, Sg4[q], vg4[q], K, inv_K, cxg, cvg, c4[q] * disc);
-                    }
-                }
-            }
-        }
-        cp_async_wait_all();  // only empty groups are left; the stages are reused next pass
-        flush();
-        // block sums of date dg (warp trees, then warps in order), published per group
-#pragma unroll
-        for (int j = 0; j < NACC; ++j) {
-            const double v = warp_sum(acc[j]);
-            if (lane == 0) s_red[warp][j] = v;
-        }
-        __syncthreads();
-        if (tid < NACC) {
-            double t = 0.0;
-            for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red[w][tid];
-            block_sums[static_cast<int64_t>(b) * NACC + tid] = t;
-            __threadfence();  // visible device-wide before this block is counted
-        }
-        __syncthreads();
-        if (p == 0 && b == withhold_block) return;  // test hook: never arrives; the others' waits run out
-        const int n_groups = (G + kLsmGroup - 1) / kLsmGroup;
-        const int grp = b / kLsmGroup;
-        const unsigned grp_size = static_cast<unsigned>(min(kLsmGroup, G - grp * kLsmGroup));
-        if (tid == 0)
-            s_group_last = atomicAdd(sync + kLsmSyncHeader + grp, 1u) == static_cast<unsigned>(p + 1) * grp_size - 1u;
-        __syncthreads();
-        if (s_group_last) {
-            __threadfence();
-            if (tid < NACC) {
-                double t = 0.0;
-                for (unsigned i = 0; i < grp_size; ++i)
-                    t += __ldcg(block_sums + static_cast<int64_t>(grp * kLsmGroup + i) * NACC + tid);
-                group_sums[grp * NACC + tid] = t;
-                __threadfence();
-            }
-            __syncthreads();
-            if (tid == 0)
-                s_all_last = atomicAdd(sync + 2, 1u) == static_cast<unsigned>(p + 1) * static_cast<unsigned>(n_groups) - 1u;
-            __syncthreads();
-            if (s_all_last) {
-                __threadfence();
-                if (tid < NACC) {
-                    double t = 0.0;
-                    for (int g = 0; g < n_groups; ++g) t += __ldcg(group_sums + g * NACC + tid);
-                    s_tot[tid] = t;
-                }
-                __syncthreads();
-                if (tid == 0) {
-                    double sums[NSUM];
-                    expand_sums<BASIS>(s_tot, sums);
-                    double c[NB];
-                    const int f = (BASIS == QK_LSM_LAGUERRE3) ? solve_reference<NB>(sums, c) : solve_scaled<NB>(sums, c);
-                    for (int i = 0; i < kMaxCoef; ++i) coeffs[dg * kMaxCoef + i] = i < NB ? c[i] : 0.0;
-                    flags[dg] = f;
-                    __threadfence();
-                    st_release_u32(sync, static_cast<unsigned>(p + 1));  // date dg's coefficients are published
-                }
-            }
-        }
-    }
-
-    // ---- final pass: date 0's decision (the payoff when it is the only date), discount
-    // to t = 0 (LSMAmerican.hpp:401-405), per-block moments; every lane takes part in the
-    // warp statistics
-    const bool init = D == 1;
-    if (!begin_pass(D - 1, 0, -1, init)) return;
-    const R K = static_cast<R>(a.K);
-    const double inv_K = 1.0 / a.K;
-    const R disc = static_cast<R>(a.disc);
-    const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);
-    const double cx = centre[0], cv = centre[1];
-    Moments mom{0.0, 0.0, 0.0, 0.0};
-    int64_t chunk = b;
-    for (int k = 0; chunk < n_chunks; ++k, chunk += G) {
-        cp_async_wait_pending<ST - 2>();
-        __syncthreads();
-        const int64_t ahead = chunk + static_cast<int64_t>(ST - 1) * G;
-        if (ahead < n_chunks) issue(0, -1, init, ahead, (k + ST - 1) % ST);
-        cp_async_commit();
-        const R *base = stage + static_cast<size_t>(k % ST) * L::kArrays * kLsmChunk;
-        const int j0 = 4 * tid;
-        const int64_t i0 = chunk * kLsmChunk + j0;
-        R val[4] = {R(0), R(0), R(0), R(0)};
-        if (i0 < a.N) {
-            R S4[4], c4[4], v4[4] = {R(0), R(0), R(0), R(0)};
-            load4(base + L::kSu * kLsmChunk + j0, S4);
-            if (!init) load4(base + L::kCf * kLsmChunk + j0, c4);
-            if (use_v) load4(base + L::kVu * kLsmChunk + j0, v4);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const R iv = lsm_intrinsic<R>(a.right, S4[q], K);
-                R c = iv;
-                if (!init) {
-                    c = c4[q] * disc;
-                    if (iv > R(0) && static_cast<double>(iv) > continuation<R, BASIS>(cu, S4[q], v4[q], K, inv_K, cx, cv))
-                        c = iv;
-                }
-                val[q] = c * disc;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            mom = chan_merge(mom, warp_moments(static_cast<double>(val[q]), i0 + q < a.N, val[q] > eps_payoff));
-    }
-    cp_async_wait_all();
-    if (lane == 0) s_mom[warp] = mom;
-    __syncthreads();
-    if (warp == 0) {
-        Moments m = lane < kLsmBlock / 32 ? s_mom[lane] : Moments{0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) m = chan_merge(m, shfl_down_moments(m, off));
-        if (lane == 0) block_moments[b] = m;
-    }
-}
-
 // ---------------------------------------------------------------- one date on caller arrays
 // The pieces of one backward step as separate operations on n paths given by the
 // caller (LSMEngine's statics, LSMAmerican.hpp:252-419): the cash flows start as the
@@ -1346,44 +989,6 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmAr
     return cudaGetLastError();
 }
 
-// Blocks of the persistent launch: every resident block slot (at most kLsmGridPerSm
-// per SM), and no more blocks than chunks.
-constexpr int kLsmGridPerSm = 2;
-
-template <class R, int BASIS>
-cudaError_t persistent_grid(int sm_count, const LsmArgs &a, int *grid) {
-    const size_t smem = lsm_sweep_smem<R, BASIS>();
-    cudaError_t e = cudaFuncSetAttribute(lsm_backward_kernel<R, BASIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_backward_kernel<R, BASIS>, kLsmBlock, smem);
-    if (e != cudaSuccess) return e;
-    const int64_t n_chunks = (a.ld + kLsmChunk - 1) / kLsmChunk;
-    *grid = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(sm_count) * std::min(std::max(per_sm, 1), kLsmGridPerSm),
-                                               std::max<int64_t>(n_chunks, 1)));
-    return cudaSuccess;
-}
-
-// The whole backward induction of one job: one cooperative launch of lsm_backward_kernel.
-// `sync` holds lsm_sync_words(grid) zeroed words; block_sums holds grid * 21 doubles
-// followed by the group sums.
-template <class R, int BASIS>
-cudaError_t enqueue_backward_persistent(cudaStream_t s, int grid, const LsmArgs &a, const R *S, const R *V, R *cf,
-                                        double *coeffs, int *flags, const double *centre, double *block_sums,
-                                        unsigned *sync, Moments *block_moments, int withhold, int64_t *launches) {
-    double *group_sums = block_sums + static_cast<int64_t>(grid) * AccTraits<BASIS>::N;
-    // the test hook withholds a block only where others are left to wait for it
-    if (withhold >= grid || grid < 2) withhold = -1;
-    void *args[] = {const_cast<LsmArgs *>(&a), const_cast<R **>(&S), const_cast<R **>(&V), &cf, &coeffs, &flags,
-                    const_cast<double **>(&centre), &block_sums, &group_sums, &sync, &block_moments, &withhold};
-    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(lsm_backward_kernel<R, BASIS>),
-                                                      dim3(static_cast<unsigned>(grid)), dim3(kLsmBlock), args,
-                                                      lsm_sweep_smem<R, BASIS>(), s);
-    ++*launches;
-    return e;
-}
-
 }  // namespace
 
 qk_status lsm_events_ensure(qk_handle *h, size_t n) {
@@ -1426,8 +1031,6 @@ void lsm_release(qk_handle *h) {
     h->lsm_fork = nullptr;
     h->lsm_task.release();
     h->lsm_centre.release();
-    h->lsm_sync.release();
-    h->h_lsm_sync.release();
     h->h_lsm.release();
     h->d_lsm_moments.release();
 }
@@ -1535,12 +1138,6 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
     QK_CUDA_LSM(cudaMemcpy(h->lsm_task.ptr, tasks.data(), nj * sizeof(TaskDev), cudaMemcpyHostToDevice));
     QK_CUDA_LSM(cudaMemcpy(h->lsm_centre.ptr, centres.data(), centres.size() * sizeof(double),
                            cudaMemcpyHostToDevice));
-    // synchronisation words of every job's persistent launch, zeroed once for the call
-    const int sync_stride = lsm_sync_words(grid);
-    if ((st = h->lsm_sync.ensure(nj * sync_stride * sizeof(unsigned))) != QK_OK) return st;
-    if ((st = h->h_lsm_sync.ensure(nj * sync_stride * sizeof(unsigned))) != QK_OK) return st;
-    QK_CUDA_LSM(cudaMemsetAsync(h->lsm_sync.ptr, 0, nj * sync_stride * sizeof(unsigned), h->stream));
-    h->lsm_sync_stride = sync_stride;
     // fork: the lanes start after the work already queued on the handle's stream
     QK_CUDA_LSM(cudaEventRecord(h->lsm_fork, h->stream));
     for (int l = 0; l < lanes; ++l) QK_CUDA_LSM(cudaStreamWaitEvent(h->lsm_stream[l], h->lsm_fork, 0));
@@ -1577,46 +1174,6 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         unsigned int *done = reinterpret_cast<unsigned int *>(
             static_cast<char *>(L.status.ptr) + ((static_cast<size_t>(lane_dates[l]) * sizeof(int) + 127) / 128) * 128);
         cudaError_t e;
-        unsigned *job_sync = static_cast<unsigned *>(h->lsm_sync.ptr) + k * sync_stride;
-        const int withhold = h->lsm_withhold_block;
-        int jgrid = grid;
-#ifndef QK_LSM_PER_DATE_LAUNCHES
-        if (D > 1) {
-            if (prec == QK_FP32) {
-                if (use_v) {
-                    e = persistent_grid<float, QK_LSM_POLY_SV>(h->sm_count, a, &jgrid);
-                    if (e == cudaSuccess)
-                        e = enqueue_backward_persistent<float, QK_LSM_POLY_SV>(
-                            s, jgrid, a, static_cast<const float *>(L.slab_S.ptr), static_cast<const float *>(L.slab_v.ptr),
-                            static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, job_sync, bm, withhold,
-                            &h->lsm_launches);
-                } else {
-                    e = persistent_grid<float, QK_LSM_LAGUERRE3>(h->sm_count, a, &jgrid);
-                    if (e == cudaSuccess)
-                        e = enqueue_backward_persistent<float, QK_LSM_LAGUERRE3>(
-                            s, jgrid, a, static_cast<const float *>(L.slab_S.ptr), nullptr,
-                            static_cast<float *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, job_sync, bm, withhold,
-                            &h->lsm_launches);
-                }
-            } else {
-                if (use_v) {
-                    e = persistent_grid<double, QK_LSM_POLY_SV>(h->sm_count, a, &jgrid);
-                    if (e == cudaSuccess)
-                        e = enqueue_backward_persistent<double, QK_LSM_POLY_SV>(
-                            s, jgrid, a, static_cast<const double *>(L.slab_S.ptr),
-                            static_cast<const double *>(L.slab_v.ptr), static_cast<double *>(L.cashflow.ptr), d_coeffs,
-                            fl, cen, bs, job_sync, bm, withhold, &h->lsm_launches);
-                } else {
-                    e = persistent_grid<double, QK_LSM_LAGUERRE3>(h->sm_count, a, &jgrid);
-                    if (e == cudaSuccess)
-                        e = enqueue_backward_persistent<double, QK_LSM_LAGUERRE3>(
-                            s, jgrid, a, static_cast<const double *>(L.slab_S.ptr), nullptr,
-                            static_cast<double *>(L.cashflow.ptr), d_coeffs, fl, cen, bs, job_sync, bm, withhold,
-                            &h->lsm_launches);
-                }
-            }
-        } else
-#endif
         if (prec == QK_FP32) {
             if (use_v)
                 e = enqueue_backward<float, QK_LSM_POLY_SV>(s, grid, h->sm_count, a,
@@ -1647,7 +1204,7 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
         LsmTaskInfo info;
         info.contract = jobs[k].contract;
         info.role = jobs[k].role;
-        info.grid = jgrid;
+        info.grid = grid;
         info.moments_base = static_cast<int64_t>(k) * grid;
         info.n_paths = b.n_paths;
         // immediate exercise value today at S0 (LSMAmerican.hpp:410-418)
@@ -1664,18 +1221,6 @@ qk_status run_lsm_contracts(qk_handle *h, Plan &plan, bool plain, std::vector<Mo
     }
     QK_CUDA_LSM(cudaMemcpyAsync(h->h_lsm.ptr, h->d_lsm_moments.ptr, nj * grid * sizeof(Moments),
                                 cudaMemcpyDeviceToHost, h->stream));
-    QK_CUDA_LSM(cudaMemcpyAsync(h->h_lsm_sync.ptr, h->lsm_sync.ptr, nj * sync_stride * sizeof(unsigned),
-                                cudaMemcpyDeviceToHost, h->stream));
-    return QK_OK;
-}
-
-qk_status lsm_check(const qk_handle *h, const Plan &plan) {
-    const unsigned *w = static_cast<const unsigned *>(h->h_lsm_sync.ptr);
-    for (size_t k = 0; k < plan.lsm_tasks.size(); ++k)
-        if (w && w[k * h->lsm_sync_stride + 1] != 0u)
-            return fail(QK_ERR_TIMEOUT, "LSM backward induction: a block's bounded wait for the next exercise "
-                                        "date's coefficients gave up (contract " +
-                                            std::to_string(plan.lsm_tasks[k].contract) + ")");
     return QK_OK;
 }
 
