@@ -93,7 +93,8 @@ def parse_args():
                     help="launch shape 'tiles_per_warp,guided_tail,paths_per_lane' instead of the autotuner")
     ap.add_argument("--paths", type=int, default=N_PATHS,
                     help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
-    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve", "kinds"], default="bates5",
+    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve", "kinds", "attribution"],
+                    default="bates5",
                     help="bates5 (default): the headline line; the others measure the remaining workloads")
     ap.add_argument("--subset", type=int, default=128, help="batch: contracts priced by both engines")
     ap.add_argument("--requests", type=int, default=20_000, help="serve: number of requests")
@@ -384,7 +385,7 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
            "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "contracts_per_s": st["contracts_per_s"],
            "path_steps_per_s": st["path_steps_per_s"], "offered_path_steps_per_s": offered / arrivals[-1],
            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
-           "lanes": lanes or 4, "wave_ms": wave_ms or 8.0,
+           "lanes": lanes or 4, "wave_ms": wave_ms or 10.0,
            "batch_all_contracts_per_s": n_requests / (t_all * 1e-3),
            "batch_all_path_steps_per_s": offered / (t_all * 1e-3),
            "served_over_batch_all": st["contracts_per_s"] / (n_requests / (t_all * 1e-3)),
@@ -513,6 +514,49 @@ def run_other_workload(args) -> None:
                               "sweep_ms": t["reduce_ms"], "forward_ms": t["device_ms"] - t["reduce_ms"]},
                     gpu_launches=args.steps * t["launches"])
         line["roofline"]["frac"] = line["roofline"]["achieved"] / line["roofline"]["peak"]
+    elif args.workload == "attribution":
+        # Where the 4096-contract mix loses against its kinds' standalone rates: the mix
+        # timed whole; each kernel kind's share of the mix (its contracts, all Greeks)
+        # timed alone; and each kind's standalone rate on one 16.8M x 252 European
+        # contract.  whole vs sum of shares = what running the kinds in one call costs
+        # or saves; shares vs standalone rates = small contracts, legs and tails.
+        g = W.batch_greeks()
+        full = W.mixed_batch()
+        tuned = [] if args.no_autotune else h.autotune(full[:256], g, reps=1)
+        qk.price_batch(full[:64], g, h)
+        with sampler:
+            t_whole = _timed(torch, ext, lambda: qk.price_batch(full, g, h), 1, flush)[0]
+            tw = h.last_timing()
+            shares = []
+            for model in (qk.HESTON, qk.BATES):
+                for scheme, sname in ((qk.EULER, "euler"), (qk.IMPLICIT_MILSTEIN, "milstein"), (qk.ANDERSEN_QE, "qe")):
+                    sub = [c for c in full if c.model == model and c.scheme == scheme]
+                    t_sub = _timed(torch, ext, lambda: qk.price_batch(sub, g, h), 1, flush)[0]
+                    big = qk.make_contract(S0=100.0, v0=0.04, r=0.03, model=model, scheme=scheme, kappa=2.0,
+                                           theta=0.04, sigma=0.3, rho=-0.7,
+                                           lambda_j=0.1 if model == qk.BATES else 0.0, mu_j=-0.05, sigma_j=0.10,
+                                           T=1.0, n_steps=N_STEPS, n_paths=N_PATHS, seed=42, precision=qk.FP32,
+                                           payoffs=[qk.payoff(qk.EUROPEAN, qk.CALL, 100.0)])
+                    qk.price_batch([big], None, h)
+                    t_big = _timed(torch, ext, lambda: qk.price_batch([big], None, h), 1, flush)[0]
+                    ps_sub = W.path_steps(sub, g)
+                    rate_big = N_PATHS * N_STEPS / (t_big * 1e-3)
+                    shares.append({"model": "bates" if model == qk.BATES else "heston", "scheme": sname,
+                                   "contracts": len(sub), "path_steps": ps_sub, "ms": t_sub,
+                                   "path_steps_per_s": ps_sub / (t_sub * 1e-3),
+                                   "standalone_path_steps_per_s": rate_big,
+                                   "share_over_standalone": ps_sub / (t_sub * 1e-3) / rate_big,
+                                   "ideal_ms": ps_sub / rate_big * 1e3})
+        ps = W.path_steps(full, g)
+        sum_ms = sum(s["ms"] for s in shares)
+        ideal_ms = sum(s["ideal_ms"] for s in shares)
+        line.update(metric="path-steps/s", value=ps / (t_whole * 1e-3), ms_per_step=t_whole, dtype="f32",
+                    config={"workload": "mixed_4096_contracts_all_greeks_seed123_attribution", "whole_ms": t_whole,
+                            "whole_paths_ms": tw["paths_ms"], "whole_merge_ms": tw["reduce_ms"],
+                            "sum_of_kind_shares_ms": sum_ms, "ideal_at_standalone_rates_ms": ideal_ms,
+                            "whole_over_ideal": t_whole / ideal_ms, "kinds": shares,
+                            "autotune": _shape_summary(tuned)},
+                    gpu_launches=tw["launches"])
     elif args.workload == "batch":
         rec = measure_batch_mix(qk, W, h, torch, ext, flush, subset=args.subset, autotune=not args.no_autotune)
         ms = rec["batched_ms"]

@@ -376,7 +376,7 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
 /* The same with all options: lanes = host threads, each with its own handle and stream,
  * whose waves run on the GPU at the same time (0 = 4); wave_ms = estimated GPU time at
  * which a lane closes the wave it is admitting, raised to the lane's share of the
- * waiting requests' estimated time when that is larger (0 = 8 ms; a wave always takes
+ * waiting requests' estimated time when that is larger (0 = 10 ms; a wave always takes
  * at least one request); hbm_budget_mib and max_batch as above.  qk_serve_start uses
  * the defaults for lanes and wave_ms. */
 typedef struct qk_serve_options {

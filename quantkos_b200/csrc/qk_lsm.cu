@@ -950,12 +950,21 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmAr
     // sweep grid: every resident block slot of the GPU (at most 4 per SM; the
     // block-sum arena holds 4 * sm_count * 32 doubles)
     const size_t smem = lsm_sweep_smem<R, BASIS>();
-    cudaError_t e = cudaFuncSetAttribute(lsm_sweep_kernel<R, BASIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    // the shared-memory attribute and the occupancy, once per device and host thread (a
+    // serving lane enqueues many small jobs; each query is a driver call)
+    static thread_local int per_sm_cache[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_sweep_kernel<R, BASIS>, kLsmBlock, smem);
-    if (e != cudaSuccess) return e;
+    int per_sm = dev >= 0 && dev < 64 ? per_sm_cache[dev] : 0;
+    if (per_sm == 0) {
+        e = cudaFuncSetAttribute(lsm_sweep_kernel<R, BASIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_sweep_kernel<R, BASIS>, kLsmBlock, smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64 && per_sm > 0) per_sm_cache[dev] = per_sm;
+    }
     // and no more blocks than chunks: a small job's empty blocks would still launch,
     // check in on the counter and have their (zero) sums folded by the last block
     const int64_t n_chunks = (a.ld + kLsmChunk - 1) / kLsmChunk;

@@ -966,6 +966,18 @@ cudaError_t preload_noalloc_kernels() {
 }
 
 int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane_mode, bool track, int block) {
+    // answered once per device, kernel variant and block size on each host thread
+    // (planning asks for every contract of every call)
+    constexpr int kDevs = 16, kVariants = 2 * 2 * 3 * 3 * 2 * 3;
+    static thread_local int cache[kDevs][kVariants] = {};
+    int dev = 0;
+    const int bidx = block == 128 ? 0 : (block == 256 ? 1 : (block == 512 ? 2 : -1));
+    int *slot = nullptr;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kDevs && bidx >= 0 && precision >= 0 &&
+        precision < 2 && model >= 0 && model < 2 && scheme >= 0 && scheme < 3 && lane_mode >= 0 && lane_mode < 3) {
+        slot = &cache[dev][((((precision * 2 + model) * 3 + scheme) * 3 + lane_mode) * 2 + (track ? 1 : 0)) * 3 + bidx];
+        if (*slot > 0) return *slot;
+    }
     int nb = 0;
     if (precision == QK_FP32)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -973,6 +985,7 @@ int price_tiles_max_blocks_per_sm(int precision, int model, int scheme, int lane
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &nb, price_kernel_for<double>(model, scheme, true, lane_mode, track), block, 0);
+    if (nb > 0 && slot) *slot = nb;
     return nb > 0 ? nb : 1;
 }
 

@@ -103,7 +103,7 @@ struct qk_server {
     int device = 0;
     size_t budget = 0, in_use = 0;
     int max_batch = 256;
-    double wave_us = 8000.0;  // GPU-time budget of one wave (the least a wave is allowed to hold)
+    double wave_us = 10000.0;  // GPU-time budget of one wave (the least a wave is allowed to hold)
     double queued_us = 0.0;   // estimated GPU time of the requests waiting for admission
     int n_lanes = 1;
     std::mutex mu;
@@ -200,7 +200,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     if (!h || !opt || !out) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
     *out = nullptr;
     if (opt->lanes < 0 || opt->lanes > 16) return qk::fail(QK_ERR_INVALID_ARG, "lanes must be in [0, 16] (0 = 4)");
-    if (opt->wave_ms < 0.0) return qk::fail(QK_ERR_INVALID_ARG, "wave_ms must be >= 0 (0 = 8 ms)");
+    if (opt->wave_ms < 0.0) return qk::fail(QK_ERR_INVALID_ARG, "wave_ms must be >= 0 (0 = 10 ms)");
     const int64_t hbm_budget_mib = opt->hbm_budget_mib;
     const int32_t max_batch = opt->max_batch;
     if (cudaSetDevice(h->device) != cudaSuccess) return qk::fail(QK_ERR_CUDA, "cudaSetDevice failed");
@@ -210,7 +210,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     s->device = h->device;
     s->budget = hbm_budget_mib > 0 ? static_cast<size_t>(hbm_budget_mib) << 20 : static_cast<size_t>(free_b * 0.8);
     s->max_batch = max_batch > 0 ? max_batch : 256;
-    s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 8000.0;
+    s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 10000.0;
     const int lanes = opt->lanes > 0 ? opt->lanes : 4;
     s->n_lanes = lanes;
     for (int i = 0; i < lanes; ++i) {

@@ -363,7 +363,7 @@ class Server:
     def __init__(self, handle: Handle | None = None, hbm_budget_mib: int = 0, max_batch: int = 256, lanes: int = 0,
                  wave_ms: float = 0.0):
         """lanes: host threads whose waves run on the GPU at once (0 = 4); wave_ms: estimated GPU time at
-        which a lane closes a wave (0 = 8 ms)."""
+        which a lane closes a wave (0 = 10 ms)."""
         self.handle = handle or default_handle()
         self._s = C.c_void_p()
         opt = L.ServeOptions(hbm_budget_mib, max_batch, lanes, wave_ms)
