@@ -352,10 +352,16 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
 
     arrivals, contracts = W.serving_stream(n_requests, rate_per_s=rate)
     srv = qk.Server(h, 0, 512, lanes, wave_ms)
-    for c in contracts[:16]:  # the lanes warm
+    # warm the server that is measured: its lanes' device arenas grow to the sizes the
+    # stream's largest requests need (one at a time, so every lane takes some), untimed;
+    # the statistics below cover the stream's own tickets only
+    by_cost = sorted(range(len(contracts)), key=lambda i: -contracts[i].n_paths * contracts[i].n_steps)
+    big = [contracts[i] for i in by_cost[:32]]
+    for tk in [srv.submit(c) for c in big]:  # all at once: the lanes share them
+        srv.poll(tk, 600_000)
+    warm = big + big + contracts[:32]
+    for c in warm[len(big):]:  # then one at a time
         srv.poll(srv.submit(c), 600_000)
-    srv.stop()
-    srv = qk.Server(h, 0, 512, lanes, wave_ms)
     tickets = []
     sampler = ClockSampler(0)
     t0 = time.perf_counter()
@@ -374,8 +380,16 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
         for tk in tickets:
             while srv.poll(tk, 1000) is None:
                 pass
-    st = srv.stats()
+    recs = [r for r in srv.records() if r["ticket"] > len(warm)]
+    reserved_mib = srv.stats()["reserved_mib"]
     srv.stop()
+    lat = sorted(r["latency_ms"] for r in recs)
+    pct = lambda q: lat[min(len(lat) - 1, int(q * (len(lat) - 1) + 0.5))]  # noqa: E731
+    span = max(r["submit_s"] + r["latency_ms"] * 1e-3 for r in recs) - min(r["submit_s"] for r in recs)
+    per_wave = {r["wave"]: r["wave_ms"] for r in recs}  # one wall time per wave
+    st = {"p50_ms": pct(0.5), "p99_ms": pct(0.99), "p999_ms": pct(0.999), "max_ms": lat[-1],
+          "contracts_per_s": len(recs) / span, "path_steps_per_s": W.path_steps(contracts) / span,
+          "batches": len(per_wave), "rejected": 0, "busy_s": sum(per_wave.values()) * 1e-3}
     offered = W.path_steps(contracts)
     # the ceiling: the batched engine pricing every request of the stream in one call
     qk.price_batch(contracts[:64], None, h)
@@ -385,7 +399,8 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
            "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "contracts_per_s": st["contracts_per_s"],
            "path_steps_per_s": st["path_steps_per_s"], "offered_path_steps_per_s": offered / arrivals[-1],
            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
-           "lanes": lanes or 4, "wave_ms": wave_ms or 10.0,
+           "lanes": lanes or 4, "wave_ms": wave_ms or 10.0, "reserved_mib": reserved_mib,
+           "warmup_requests": len(warm),
            "batch_all_contracts_per_s": n_requests / (t_all * 1e-3),
            "batch_all_path_steps_per_s": offered / (t_all * 1e-3),
            "served_over_batch_all": st["contracts_per_s"] / (n_requests / (t_all * 1e-3)),
@@ -488,6 +503,10 @@ def run_other_workload(args) -> None:
                             "algorithmic_ops": {"issue": ISSUE_OPS, "sfu": SFU_OPS}},
                     gpu_launches=None)
     elif args.workload == "lsm":
+        pk_file = ROOT / "MEASURED_PEAKS.json"
+        measured = json.loads(pk_file.read_text()).get("hbm_gbs") if pk_file.exists() else None
+        hbm_peak = (measured, "measured copy bandwidth (MEASURED_PEAKS.json)") if measured else \
+            (6650.0, "fallback 6.65 TB/s (no measured peak file)")
         c32 = W.american_lsm(precision=qk.FP32)
         c64 = W.american_lsm(precision=qk.FP64)
         for _ in range(args.warmup):
@@ -508,8 +527,7 @@ def run_other_workload(args) -> None:
                             "std_error": r32["std_error"], "price_fp64": r64["price"], "std_error_fp64": r64["std_error"],
                             "fp64_plain_ms": t64, "speedup_vs_fp64_plain": t64 / ms},
                     roofline={"bound": "hbm", "achieved": sweep_bytes / (t["reduce_ms"] * 1e-3) / 1e9,
-                              "peak": json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs")
-                              if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0,
+                              "peak": hbm_peak[0], "peak_source": hbm_peak[1],
                               "unit": "GB/s", "kernel": "LSM backward sweep (all dates)",
                               "sweep_ms": t["reduce_ms"], "forward_ms": t["device_ms"] - t["reduce_ms"]},
                     gpu_launches=args.steps * t["launches"])
@@ -626,7 +644,7 @@ def main() -> None:
     elif not args.no_autotune:
         rep = h.autotune([contract], None, reps=1)[0]
         tuned = {"tiles_per_warp": rep["tiles_per_warp"], "guided_tail": rep["guided_tail"],
-                 "paths_per_lane": rep["paths_per_lane"],
+                 "paths_per_lane": rep["paths_per_lane"], "block_size": rep["block_size"],
                  "best_ms": rep["best_ms"], "default_ms": rep["default_ms"]}
 
     # ---- value: descriptors resident in HBM, K device-timed pricings

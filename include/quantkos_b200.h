@@ -367,23 +367,30 @@ qk_status qk_run_config(qk_handle *h, const qk_config *c, qk_result *out, double
 typedef struct qk_server qk_server;
 typedef struct qk_serve_stats {
     int64_t submitted, completed, rejected;
-    double p50_ms, p99_ms, p999_ms, max_ms;
+    double p50_ms, p99_ms, p999_ms, max_ms; /* over the most recent 1,048,576 requests */
     double contracts_per_s, path_steps_per_s;
     int64_t batches;
     double busy_s;
+    int64_t reserved_mib; /* HBM the server holds in the device's memory pool */
 } qk_serve_stats;
 qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch, qk_server **out);
 /* The same with all options: lanes = host threads, each with its own handle and stream,
  * whose waves run on the GPU at the same time (0 = 4); wave_ms = estimated GPU time at
  * which a lane closes the wave it is admitting, raised to the lane's share of the
  * waiting requests' estimated time when that is larger (0 = 10 ms; a wave always takes
- * at least one request); hbm_budget_mib and max_batch as above.  qk_serve_start uses
- * the defaults for lanes and wave_ms. */
+ * at least one request); reserve_mib = HBM mapped into the device's memory pool at the
+ * start and held until qk_serve_stop, from which the lanes' buffers grow (0 = the
+ * budget; -1 = none; mapping new memory while lanes run blocks every lane's driver
+ * calls for up to hundreds of milliseconds).  A default reservation that does not fit
+ * is skipped; an explicit one that does not fit fails with QK_ERR_CAPACITY.
+ * hbm_budget_mib and max_batch as above.  qk_serve_start uses the defaults for lanes,
+ * wave_ms and reserve_mib. */
 typedef struct qk_serve_options {
     int64_t hbm_budget_mib;
     int32_t max_batch;
     int32_t lanes;
     double wave_ms;
+    int64_t reserve_mib;
 } qk_serve_options;
 qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server **out);
 qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g, int64_t *ticket);
@@ -394,6 +401,22 @@ qk_status qk_serve_poll(qk_server *s, int64_t ticket, int32_t wait_ms, int32_t *
  * completion (*cancelled = 0).  Thread-safe. */
 qk_status qk_serve_cancel(qk_server *s, int64_t ticket, int32_t *cancelled);
 qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out);
+/* Per-request accounting of the most recent completed requests (at most 1,048,576, the
+ * window the latency percentiles of qk_serve_stats_get also cover), oldest first: copies
+ * up to `capacity` records and sets *count to the number held. */
+typedef struct qk_serve_record {
+    int64_t ticket;
+    int64_t wave;          /* the wave it was priced in, numbered in order of admission */
+    int32_t lane;          /* the lane that priced that wave */
+    int32_t wave_requests; /* requests in that wave */
+    double submit_s;       /* submit time, seconds after the server's first submit */
+    double admit_ms;       /* from submit to the start of its wave */
+    double latency_ms;     /* from submit to completion */
+    double wave_ms;        /* wall time of its wave (plan, upload, kernels, results) */
+    double wave_est_ms;    /* estimated GPU time of its wave */
+    double est_ms;         /* estimated GPU time of the request */
+} qk_serve_record;
+qk_status qk_serve_records(qk_server *s, qk_serve_record *out, int64_t capacity, int64_t *count);
 qk_status qk_serve_stop(qk_server *s);
 
 #ifdef __cplusplus

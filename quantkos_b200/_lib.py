@@ -95,7 +95,7 @@ class ServeStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("rejected", C.c_int64),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p999_ms", C.c_double), ("max_ms", C.c_double),
                 ("contracts_per_s", C.c_double), ("path_steps_per_s", C.c_double),
-                ("batches", C.c_int64), ("busy_s", C.c_double)]
+                ("batches", C.c_int64), ("busy_s", C.c_double), ("reserved_mib", C.c_int64)]
 
 
 class Config(C.Structure):
@@ -119,8 +119,15 @@ class Config(C.Structure):
     ]
 
 
+class ServeRecord(C.Structure):
+    _fields_ = [("ticket", C.c_int64), ("wave", C.c_int64), ("lane", C.c_int32), ("wave_requests", C.c_int32),
+                ("submit_s", C.c_double), ("admit_ms", C.c_double), ("latency_ms", C.c_double),
+                ("wave_ms", C.c_double), ("wave_est_ms", C.c_double), ("est_ms", C.c_double)]
+
+
 class ServeOptions(C.Structure):
-    _fields_ = [("hbm_budget_mib", C.c_int64), ("max_batch", C.c_int32), ("lanes", C.c_int32), ("wave_ms", C.c_double)]
+    _fields_ = [("hbm_budget_mib", C.c_int64), ("max_batch", C.c_int32), ("lanes", C.c_int32), ("wave_ms", C.c_double),
+                ("reserve_mib", C.c_int64)]
 
 
 _P = C.POINTER
@@ -165,6 +172,7 @@ SIGNATURES = {
     "qk_run_config": (C.c_int, [_VP, _P(Config), _P(Result), _P(C.c_double)]),
     "qk_serve_start": (C.c_int, [_VP, C.c_int64, C.c_int32, _P(_VP)]),
     "qk_serve_start_ex": (C.c_int, [_VP, _P(ServeOptions), _P(_VP)]),
+    "qk_serve_records": (C.c_int, [_VP, _P(ServeRecord), C.c_int64, _P(C.c_int64)]),
     "qk_serve_submit": (C.c_int, [_VP, _P(Contract), _P(Greeks), _P(C.c_int64)]),
     "qk_serve_poll": (C.c_int, [_VP, C.c_int64, C.c_int32, _P(C.c_int32), _P(Result)]),
     "qk_serve_cancel": (C.c_int, [_VP, C.c_int64, _P(C.c_int32)]),

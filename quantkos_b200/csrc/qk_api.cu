@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -286,28 +287,75 @@ int choose_ppt(int64_t n_paths, int64_t total_paths_all, int sm_count, int tiles
     return static_cast<int>(ppt);
 }
 
+// ---------------------------------------------------------------- the device pool
+namespace {
+std::mutex g_pool_mu;
+size_t g_pool_keep[64] = {};  // bytes the live servers hold in each device's pool
+}  // namespace
+
+qk_status pool_reserve(int device, cudaStream_t s, size_t bytes) {
+    if (bytes == 0) return QK_OK;
+    if (device < 0 || device >= 64) return fail(QK_ERR_INVALID_ARG, "device index out of range");
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QK_ERR_CAPACITY, "cannot reserve " + std::to_string(bytes >> 20) + " MiB in the device pool");
+    }
+    QK_CUDA_TRY(cudaFreeAsync(p, s));
+    QK_CUDA_TRY(cudaStreamSynchronize(s));
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    g_pool_keep[device] += bytes;
+    return QK_OK;
+}
+
+void pool_release(int device, size_t bytes) {
+    if (device < 0 || device >= 64) return;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        g_pool_keep[device] -= std::min(bytes, g_pool_keep[device]);
+    }
+    pool_trim(device);
+}
+
+void pool_trim(int device) {
+    if (device < 0 || device >= 64) return;
+    cudaMemPool_t pool;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, g_pool_keep[device]);
+}
+
 // ---------------------------------------------------------------- device arenas
 qk_status DevArena::ensure(size_t bytes) {
     if (bytes <= cap) return QK_OK;
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    cap = 0;
-    const size_t want = std::max<size_t>(bytes, 4096);
-    QK_CUDA_TRY(cudaMalloc(&ptr, want));
+    const size_t want = std::max<size_t>({bytes, cap + cap / 2, 4096});
+    if (stream) {
+        if (ptr) cudaFreeAsync(ptr, stream);
+        ptr = nullptr;
+        cap = 0;
+        QK_CUDA_TRY(cudaMallocAsync(&ptr, want, stream));
+    } else {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+        QK_CUDA_TRY(cudaMalloc(&ptr, want));
+    }
     cap = want;
     return QK_OK;
 }
 void DevArena::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (stream) cudaFreeAsync(ptr, stream);
+        else cudaFree(ptr);
+    }
     ptr = nullptr;
     cap = 0;
 }
 qk_status HostArena::ensure(size_t bytes) {
     if (bytes <= cap) return QK_OK;
+    const size_t want = std::max<size_t>({bytes, cap + cap / 2, size_t(1) << 20});
     if (ptr) cudaFreeHost(ptr);
     ptr = nullptr;
     cap = 0;
-    const size_t want = std::max<size_t>(bytes, 4096);
     QK_CUDA_TRY(cudaMallocHost(&ptr, want));
     cap = want;
     return QK_OK;
@@ -749,6 +797,18 @@ qk_status qk_create(int32_t device, qk_handle **out) {
     cudaDeviceProp prop;
     QK_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) return fail(QK_ERR_UNSUPPORTED, std::string("built for sm_100a; device is ") + prop.name);
+    {
+        // every kernel's device code is loaded once per device, before any pricing call
+        static std::mutex mu;
+        static bool loaded[64] = {};
+        std::lock_guard<std::mutex> lk(mu);
+        if (device < 64 && !loaded[device]) {
+            cudaError_t e = preload_path_kernels();
+            if (e == cudaSuccess) e = preload_lsm_kernels();
+            if (e != cudaSuccess) return fail(QK_ERR_CUDA, std::string("loading the kernels: ") + cudaGetErrorString(e));
+            loaded[device] = true;
+        }
+    }
     qk_handle *h = new qk_handle();
     h->device = device;
     h->sm_count = prop.multiProcessorCount;
@@ -762,6 +822,21 @@ qk_status qk_create(int32_t device, qk_handle **out) {
     if (!ok) {
         delete h;
         return fail(QK_ERR_CUDA, "stream/event creation failed");
+    }
+    // device arenas grow stream-ordered on the handle's stream (the LSM working sets are
+    // used by the LSM streams only after they fork from it); the device's memory pool
+    // keeps freed blocks for reuse instead of returning them at every synchronization
+    for (qk::DevArena *a : {&h->d_tasks, &h->d_prefix, &h->d_partials, &h->d_moments, &h->d_cursor, &h->d_trace,
+                            &h->d_chunks, &h->d_lsm_moments, &h->lsm_task, &h->lsm_centre})
+        a->stream = h->stream;
+    for (int l = 0; l < kLsmLanes; ++l)
+        for (qk::DevArena *a : {&h->lsm[l].slab_S, &h->lsm[l].slab_v, &h->lsm[l].cashflow, &h->lsm[l].block_sums,
+                                &h->lsm[l].coeffs, &h->lsm[l].status})
+            a->stream = h->stream;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     *out = h;
     return QK_OK;
@@ -782,6 +857,8 @@ qk_status qk_destroy(qk_handle *h) {
     h->d_trace.release();
     h->h_tasks.release();
     h->h_moments.release();
+    cudaStreamSynchronize(h->stream);  // the stream-ordered frees above have completed
+    pool_trim(h->device);  // unused blocks back, down to what live servers hold
     cudaEventDestroy(h->ev_start);
     cudaEventDestroy(h->ev_paths0);
     cudaEventDestroy(h->ev_paths1);

@@ -12,15 +12,21 @@
 namespace qk {
 
 // Grow-only device allocation owned by a handle (replaces the per-run Kokkos
-// Views of PathsMCBatchMem / BackwardLSMMemory: allocated once, reused).
+// Views of PathsMCBatchMem / BackwardLSMMemory: allocated once, reused).  With a
+// stream set, growth is stream-ordered (cudaFreeAsync / cudaMallocAsync on that
+// stream, from the device's memory pool), so growing one handle's arena does not
+// synchronize the device and stall other handles' work; it grows by at least half
+// its size, so growth events are few.
 struct DevArena {
     void *ptr = nullptr;
     size_t cap = 0;
+    cudaStream_t stream = nullptr;  // the owning handle's stream (nullptr: cudaMalloc / cudaFree)
     qk_status ensure(size_t bytes);
     void release();
 };
 
-// Grow-only pinned host staging buffer.
+// Grow-only pinned host staging buffer (at least 1 MiB, grows by at least half its size:
+// pinning host memory is slow and can stall other work, so it happens rarely).
 struct HostArena {
     void *ptr = nullptr;
     size_t cap = 0;
@@ -124,6 +130,16 @@ std::vector<int> roles_for(const qk_greeks *g, double T);
 // Plan, run and assemble a set of contracts; `gs` holds one Greeks request per
 // contract (or NULL).  Used by qk_price_* and by the serving lanes.
 qk_status price_contracts(qk_handle *h, const qk_contract *c, int32_t n, const qk_greeks *gs, qk_result *out, bool plain);
+
+// Memory held in a device's default pool (whose release threshold the handles raise so
+// that it keeps what it has mapped): pool_reserve maps `bytes` into it once (allocate and
+// free on `s`) and adds them to what handle destruction trims the pool down to; a
+// server reserves its budget this way, so that its lanes' arena growth is served from
+// memory the pool holds instead of mapping new memory, which blocks every other lane's
+// driver calls while it runs.  pool_release gives them back and trims the pool.
+qk_status pool_reserve(int device, cudaStream_t s, size_t bytes);
+void pool_release(int device, size_t bytes);
+void pool_trim(int device);
 
 // Every path's leg-0 payoff (undiscounted, normalised) of a contract, on the host.
 qk_status payoffs_dump(qk_handle *h, const qk_contract &c, std::vector<double> &out);

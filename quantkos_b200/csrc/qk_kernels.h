@@ -59,6 +59,12 @@ bool price_tiles_block_ok(int precision, int block);
 // every model and scheme, with and without path state) and of the one-block-per-task
 // merge, without launching anything.
 cudaError_t preload_noalloc_kernels();
+// Load the device code of every kernel of the engine on the current device (path and
+// merge kernels; the LSM kernels).  With lazy module loading, a kernel's first launch
+// loads its code and can synchronize the context while other streams' kernels run;
+// handles preload everything once per device so that no pricing call pays that.
+cudaError_t preload_path_kernels();
+cudaError_t preload_lsm_kernels();
 // Times a kernel of independent ex2.approx chains; returns its duration and MUFU op count.
 cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEvent_t e0, cudaEvent_t e1, float *ms,
                              double *ops);

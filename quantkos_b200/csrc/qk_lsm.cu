@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -926,6 +927,27 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_date_update_kernel(int right, i
     cf[i] = static_cast<double>(out);
 }
 
+template <class R, int BASIS>
+static cudaError_t preload_lsm_kernels_of() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, lsm_sweep_kernel<R, BASIS>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, lsm_final_kernel<R, BASIS>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, lsm_date_sums_kernel<R, BASIS>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, lsm_date_update_kernel<R, BASIS>);
+    return e;
+}
+
+cudaError_t preload_lsm_kernels() {
+    cudaFuncAttributes fa;
+    cudaError_t e = preload_lsm_kernels_of<float, QK_LSM_LAGUERRE3>();
+    if (e == cudaSuccess) e = preload_lsm_kernels_of<float, QK_LSM_POLY_SV>();
+    if (e == cudaSuccess) e = preload_lsm_kernels_of<double, QK_LSM_LAGUERRE3>();
+    if (e == cudaSuccess) e = preload_lsm_kernels_of<double, QK_LSM_POLY_SV>();
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, lsm_date_solve_kernel<QK_LSM_LAGUERRE3>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, lsm_date_solve_kernel<QK_LSM_POLY_SV>);
+    return e;
+}
+
 // ---------------------------------------------------------------- host side
 namespace {
 
@@ -950,20 +972,20 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmAr
     // sweep grid: every resident block slot of the GPU (at most 4 per SM; the
     // block-sum arena holds 4 * sm_count * 32 doubles)
     const size_t smem = lsm_sweep_smem<R, BASIS>();
-    // the shared-memory attribute and the occupancy, once per device and host thread (a
+    // the shared-memory attribute (context-wide) and the occupancy, once per device (a
     // serving lane enqueues many small jobs; each query is a driver call)
-    static thread_local int per_sm_cache[64] = {};
+    static std::atomic<int> per_sm_cache[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    int per_sm = dev >= 0 && dev < 64 ? per_sm_cache[dev] : 0;
+    int per_sm = dev >= 0 && dev < 64 ? per_sm_cache[dev].load(std::memory_order_relaxed) : 0;
     if (per_sm == 0) {
         e = cudaFuncSetAttribute(lsm_sweep_kernel<R, BASIS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_sweep_kernel<R, BASIS>, kLsmBlock, smem);
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64 && per_sm > 0) per_sm_cache[dev] = per_sm;
+        if (dev >= 0 && dev < 64 && per_sm > 0) per_sm_cache[dev].store(per_sm, std::memory_order_relaxed);
     }
     // and no more blocks than chunks: a small job's empty blocks would still launch,
     // check in on the counter and have their (zero) sums folded by the last block
@@ -1001,7 +1023,9 @@ cudaError_t enqueue_backward(cudaStream_t s, int grid, int sm_count, const LsmAr
 }  // namespace
 
 qk_status lsm_events_ensure(qk_handle *h, size_t n) {
-    while (h->lsm_events.size() < n) {
+    // grown geometrically: creating events takes the driver's lock, which other lanes' calls wait on
+    const size_t want = h->lsm_events.size() >= n ? n : std::max<size_t>({n, 2 * h->lsm_events.size(), 48});
+    while (h->lsm_events.size() < want) {
         cudaEvent_t e;
         if (cudaEventCreate(&e) != cudaSuccess) return fail(QK_ERR_CUDA, "LSM: cudaEventCreate failed");
         h->lsm_events.push_back(e);

@@ -952,6 +952,37 @@ cudaError_t launch_sfu_probe(cudaStream_t s, int sm_count, float *sink, cudaEven
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
+// Loads the device code of every kernel in this file on the current device.
+template <class R>
+static cudaError_t preload_path_kernels_of() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaSuccess;
+    for (int model = 0; model < 2 && e == cudaSuccess; ++model)
+        for (int scheme = 0; scheme < 3 && e == cudaSuccess; ++scheme) {
+            for (int uk = 0; uk < 2 && e == cudaSuccess; ++uk)
+                for (int lane = 0; lane < 3 && e == cudaSuccess; ++lane)
+                    for (int trk = 0; trk < 2 && e == cudaSuccess; ++trk)
+                        e = cudaFuncGetAttributes(&fa, price_kernel_for<R>(model, scheme, uk != 0, lane, trk != 0));
+            if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, slab_kernel_for<R>(model, scheme));
+            if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, slab_two_kernel_for<R>(model, scheme));
+        }
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, payoff_paths_kernel<R>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, payoff_trace_kernel<R>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, step_trace_kernel<R>);
+    return e;
+}
+
+cudaError_t preload_path_kernels() {
+    cudaFuncAttributes fa;
+    cudaError_t e = preload_path_kernels_of<float>();
+    if (e == cudaSuccess) e = preload_path_kernels_of<double>();
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, merge_tasks_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, merge_chunks_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, merge_task_chunks_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, sfu_probe_kernel);
+    return e;
+}
+
 cudaError_t preload_noalloc_kernels() {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, merge_tasks_kernel);

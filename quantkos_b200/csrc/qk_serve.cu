@@ -106,6 +106,7 @@ struct qk_server {
     double wave_us = 10000.0;  // GPU-time budget of one wave (the least a wave is allowed to hold)
     double queued_us = 0.0;   // estimated GPU time of the requests waiting for admission
     int n_lanes = 1;
+    size_t reserved = 0;  // bytes held in the device pool for the lanes (pool_reserve)
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request> queue;
@@ -114,15 +115,19 @@ struct qk_server {
     bool stop = false;
     std::vector<std::thread> lanes;
     std::vector<qk_handle *> handles;
-    // statistics
-    std::vector<double> latencies;
+    // statistics; the per-request records are a window over the most recent
+    // kRecordWindow completed requests (a ring once full: rec_head is its oldest)
+    static constexpr size_t kRecordWindow = size_t(1) << 20;
+    std::vector<qk_serve_record> records;
+    size_t rec_head = 0;
+    int64_t next_wave = 0;
     int64_t submitted = 0, completed = 0, rejected = 0, batches = 0;
     double path_steps = 0.0, busy_s = 0.0;
     bool have_first = false;
     Clock::time_point t_first, t_last;
 };
 
-static void lane_loop(qk_server *s, qk_handle *h) {
+static void lane_loop(qk_server *s, qk_handle *h, int lane) {
     std::vector<Request> batch;
     std::vector<qk_contract> cs;
     std::vector<qk_greeks> gs;
@@ -130,6 +135,8 @@ static void lane_loop(qk_server *s, qk_handle *h) {
     for (;;) {
         batch.clear();
         size_t bytes = 0;
+        double est = 0.0;
+        int64_t wave = 0;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             for (;;) {
@@ -137,7 +144,7 @@ static void lane_loop(qk_server *s, qk_handle *h) {
                 // wave size: the budget, or this lane's share of the backlog when that is larger
                 // (small waves while the queue is short, large ones under load)
                 const double cap = std::max(s->wave_us, s->queued_us / s->n_lanes);
-                double est = 0.0;
+                est = 0.0;
                 while (!s->queue.empty() && static_cast<int>(batch.size()) < s->max_batch &&
                        s->in_use + bytes + s->queue.front().bytes <= s->budget &&
                        (batch.empty() || est + s->queue.front().est_us <= cap)) {
@@ -152,6 +159,7 @@ static void lane_loop(qk_server *s, qk_handle *h) {
                 s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
             }
             s->in_use += bytes;
+            wave = s->next_wave++;
         }
         cs.resize(batch.size());
         gs.resize(batch.size());
@@ -174,7 +182,23 @@ static void lane_loop(qk_server *s, qk_handle *h) {
                 f.r = rs[i];
                 if (st != QK_OK) f.r.status = st;
                 f.latency_ms = std::chrono::duration<double, std::milli>(t1 - batch[i].t_submit).count();
-                s->latencies.push_back(f.latency_ms);
+                qk_serve_record rec;
+                rec.ticket = batch[i].ticket;
+                rec.wave = wave;
+                rec.lane = lane;
+                rec.wave_requests = static_cast<int32_t>(batch.size());
+                rec.submit_s = std::chrono::duration<double>(batch[i].t_submit - s->t_first).count();
+                rec.admit_ms = std::chrono::duration<double, std::milli>(t0 - batch[i].t_submit).count();
+                rec.latency_ms = f.latency_ms;
+                rec.wave_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+                rec.wave_est_ms = est * 1e-3;
+                rec.est_ms = batch[i].est_us * 1e-3;
+                if (s->records.size() < qk_server::kRecordWindow) {
+                    s->records.push_back(rec);
+                } else {
+                    s->records[s->rec_head] = rec;
+                    s->rec_head = (s->rec_head + 1) % qk_server::kRecordWindow;
+                }
                 s->completed++;
                 if (st == QK_OK) s->path_steps += rs[i].path_steps;
                 s->done[batch[i].ticket] = f;
@@ -201,6 +225,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     *out = nullptr;
     if (opt->lanes < 0 || opt->lanes > 16) return qk::fail(QK_ERR_INVALID_ARG, "lanes must be in [0, 16] (0 = 4)");
     if (opt->wave_ms < 0.0) return qk::fail(QK_ERR_INVALID_ARG, "wave_ms must be >= 0 (0 = 10 ms)");
+    if (opt->reserve_mib < -1) return qk::fail(QK_ERR_INVALID_ARG, "reserve_mib must be >= -1 (0 = the budget, -1 = none)");
     const int64_t hbm_budget_mib = opt->hbm_budget_mib;
     const int32_t max_batch = opt->max_batch;
     if (cudaSetDevice(h->device) != cudaSuccess) return qk::fail(QK_ERR_CUDA, "cudaSetDevice failed");
@@ -213,11 +238,22 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 10000.0;
     const int lanes = opt->lanes > 0 ? opt->lanes : 4;
     s->n_lanes = lanes;
+    const size_t reserve = opt->reserve_mib > 0 ? static_cast<size_t>(opt->reserve_mib) << 20
+                           : opt->reserve_mib == 0 ? s->budget : 0;
+    if (reserve > 0) {
+        const qk_status st = qk::pool_reserve(h->device, h->stream, reserve);
+        if (st == QK_OK) s->reserved = reserve;
+        else if (opt->reserve_mib > 0) {
+            delete s;
+            return st;
+        }
+    }
     for (int i = 0; i < lanes; ++i) {
         qk_handle *lh = nullptr;
         const qk_status st = qk_create(h->device, &lh);
         if (st != QK_OK) {
             for (qk_handle *x : s->handles) qk_destroy(x);
+            qk::pool_release(s->device, s->reserved);
             delete s;
             return st;
         }
@@ -229,7 +265,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
         lh->tune_block = h->tune_block;
         s->handles.push_back(lh);
     }
-    for (qk_handle *lh : s->handles) s->lanes.emplace_back(lane_loop, s, lh);
+    for (size_t i = 0; i < s->handles.size(); ++i) s->lanes.emplace_back(lane_loop, s, s->handles[i], static_cast<int>(i));
     *out = s;
     return QK_OK;
 }
@@ -313,8 +349,10 @@ qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out) {
     out->rejected = s->rejected;
     out->batches = s->batches;
     out->busy_s = s->busy_s;
-    if (!s->latencies.empty()) {
-        std::vector<double> l = s->latencies;
+    out->reserved_mib = static_cast<int64_t>(s->reserved >> 20);
+    if (!s->records.empty()) {
+        std::vector<double> l(s->records.size());
+        for (size_t i = 0; i < l.size(); ++i) l[i] = s->records[i].latency_ms;
         std::sort(l.begin(), l.end());
         auto pct = [&](double p) { return l[std::min(l.size() - 1, static_cast<size_t>(p * (l.size() - 1) + 0.5))]; };
         out->p50_ms = pct(0.50);
@@ -330,6 +368,16 @@ qk_status qk_serve_stats_get(qk_server *s, qk_serve_stats *out) {
     return QK_OK;
 }
 
+qk_status qk_serve_records(qk_server *s, qk_serve_record *out, int64_t capacity, int64_t *count) {
+    if (!s || !count || (capacity > 0 && !out)) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const size_t n = s->records.size();
+    const size_t m = std::min(n, static_cast<size_t>(std::max<int64_t>(capacity, 0)));
+    for (size_t i = 0; i < m; ++i) out[i] = s->records[(s->rec_head + i) % n];
+    *count = static_cast<int64_t>(n);
+    return QK_OK;
+}
+
 qk_status qk_serve_stop(qk_server *s) {
     if (!s) return QK_OK;
     {
@@ -339,6 +387,7 @@ qk_status qk_serve_stop(qk_server *s) {
     s->cv_work.notify_all();
     for (auto &t : s->lanes) t.join();
     for (qk_handle *h : s->handles) qk_destroy(h);
+    qk::pool_release(s->device, s->reserved);
     delete s;
     return QK_OK;
 }

@@ -361,12 +361,13 @@ class Server:
     """Continuous-batching request loop (qk_serve_*)."""
 
     def __init__(self, handle: Handle | None = None, hbm_budget_mib: int = 0, max_batch: int = 256, lanes: int = 0,
-                 wave_ms: float = 0.0):
+                 wave_ms: float = 0.0, reserve_mib: int = 0):
         """lanes: host threads whose waves run on the GPU at once (0 = 4); wave_ms: estimated GPU time at
-        which a lane closes a wave (0 = 10 ms)."""
+        which a lane closes a wave (0 = 10 ms); reserve_mib: HBM mapped into the device pool at the start and
+        held until stop, from which the lanes' buffers grow (0 = the budget, -1 = none)."""
         self.handle = handle or default_handle()
         self._s = C.c_void_p()
-        opt = L.ServeOptions(hbm_budget_mib, max_batch, lanes, wave_ms)
+        opt = L.ServeOptions(hbm_budget_mib, max_batch, lanes, wave_ms, reserve_mib)
         check(L.lib().qk_serve_start_ex(self.handle.ptr, C.byref(opt), C.byref(self._s)), "qk_serve_start_ex")
 
     def submit(self, contract: L.Contract, greeks: L.Greeks | None = None) -> int:
@@ -386,6 +387,14 @@ class Server:
         c = C.c_int32()
         check(L.lib().qk_serve_cancel(self._s, ticket, C.byref(c)), "qk_serve_cancel")
         return bool(c.value)
+
+    def records(self) -> list[dict]:
+        """Per-request accounting of the completed requests (qk_serve_records)."""
+        n = C.c_int64()
+        check(L.lib().qk_serve_records(self._s, None, 0, C.byref(n)), "qk_serve_records")
+        arr = (L.ServeRecord * max(n.value, 1))()
+        check(L.lib().qk_serve_records(self._s, arr, n.value, C.byref(n)), "qk_serve_records")
+        return [{f: getattr(arr[i], f) for f, _ in L.ServeRecord._fields_} for i in range(n.value)]
 
     def stats(self) -> dict:
         s = L.ServeStats()

@@ -42,10 +42,11 @@ def test_struct_layouts_match_c(tmp_path, qk):
         #include <stddef.h>
         #include "quantkos_b200.h"
         int main(void) {
-          printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(qk_contract), sizeof(qk_config),
+          printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(qk_contract), sizeof(qk_config),
                  sizeof(qk_result), sizeof(qk_greeks), sizeof(qk_timing), sizeof(qk_serve_stats), sizeof(qk_payoff),
                  offsetof(qk_contract, payoffs), offsetof(qk_config, paths_file), offsetof(qk_result, p),
-                 sizeof(qk_tune_report), offsetof(qk_tune_report, best_ms));
+                 sizeof(qk_tune_report), offsetof(qk_tune_report, best_ms), sizeof(qk_serve_options),
+                 offsetof(qk_serve_options, reserve_mib), sizeof(qk_serve_record), offsetof(qk_serve_record, est_ms));
           return 0;
         }"""))
     exe = tmp_path / "sz"
@@ -53,7 +54,8 @@ def test_struct_layouts_match_c(tmp_path, qk):
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(L.Contract), C.sizeof(L.Config), C.sizeof(L.Result), C.sizeof(L.Greeks), C.sizeof(L.Timing),
             C.sizeof(L.ServeStats), C.sizeof(L.Payoff), L.Contract.payoffs.offset, L.Config.paths_file.offset,
-            L.Result.p.offset, C.sizeof(L.TuneReport), L.TuneReport.best_ms.offset]
+            L.Result.p.offset, C.sizeof(L.TuneReport), L.TuneReport.best_ms.offset, C.sizeof(L.ServeOptions),
+            L.ServeOptions.reserve_mib.offset, C.sizeof(L.ServeRecord), L.ServeRecord.est_ms.offset]
     assert got == want
 
 

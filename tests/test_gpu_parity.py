@@ -127,6 +127,38 @@ def test_launch_shape_invariance(qk, handle):
     assert plain == pytest.approx(alone, rel=1e-13)
 
 
+def test_block_size_changes_no_result(qk, handle):
+    """Threads per block of the pricing kernel (128, 256, 512 in FP32; 128, 256 in FP64) only
+    change which warps run the tiles: every tile covers the same paths and writes the same
+    record, so every price, standard error and Greek is bit for bit the same; the autotuner's
+    choice reports a valid block size."""
+    legs = [qk.payoff(qk.EUROPEAN, qk.CALL, 100.0), qk.payoff(qk.ASIAN, qk.PUT, 95.0),
+            qk.payoff(qk.BARRIER_UP_OUT, qk.CALL, 100.0, 125.0)]
+    g = qk.make_greeks(qk.GREEK_ALL, bump_S_rel=0.01, bump_vol=0.02, bump_r_abs=1e-3, bump_T_abs=2 / 365)
+    key = lambda r: [(leg[f] for f in ("price", "std_error", "delta", "gamma", "vega", "vanna", "theta"))
+                     for leg in r["legs"]]
+    for prec, blocks in ((qk.FP32, (128, 256, 512)), (qk.FP64, (128, 256))):
+        ks = [qk.make_contract(model=qk.BATES, scheme=s, lambda_j=0.3, mu_j=-0.1, sigma_j=0.1, n_paths=n,
+                               n_steps=40, seed=17, stream=i, precision=prec, payoffs=legs)
+              for i, (s, n) in enumerate(((qk.ANDERSEN_QE, 400_003), (qk.EULER, 77_777), (qk.IMPLICIT_MILSTEIN, 150_000)))]
+        results = []
+        try:
+            for b in blocks:
+                for s in (qk.EULER, qk.IMPLICIT_MILSTEIN, qk.ANDERSEN_QE):
+                    handle.tune_set(prec, qk.BATES, s, 24, False, 2 if prec == qk.FP32 else 1, block_size=b)
+                rs = qk.price_batch(ks, g, handle)
+                results.append([[list(x) for x in key(r)] for r in rs])
+        finally:
+            handle.tune_reset()
+        for other in results[1:]:
+            assert other == results[0]
+    with pytest.raises(qk.QuantKosInvalidArgument):
+        handle.tune_set(qk.FP64, qk.HESTON, qk.EULER, 24, False, 1, block_size=512)
+    rep = handle.autotune([qk.make_contract(n_paths=200_000, n_steps=32, precision=qk.FP32)], None, reps=1)
+    assert rep[0]["block_size"] in (128, 256, 512)
+    handle.tune_reset()
+
+
 def test_greeks_match_oracle(qk, handle, oracle):
     g = qk.make_greeks(qk.GREEK_ALL, bump_S_rel=0.01, bump_vol=0.02, bump_r_abs=0.001, bump_T_abs=7 / 365)
     for otype in (qk.EUROPEAN, qk.ASIAN, qk.BARRIER_DOWN_OUT):

@@ -200,6 +200,31 @@ def test_server_admission_rejects_oversized(qk, handle):
         assert srv.stats()["rejected"] == 1
 
 
+def test_server_reserves_pool_memory(qk, handle):
+    """The server maps its reservation into the device pool at the start (0 = the budget, -1 =
+    none, else the MiB given), holds it while it runs and gives it back at the stop; an
+    explicit reservation that cannot fit fails with QK_ERR_CAPACITY and leaves nothing held."""
+    import torch
+    from quantkos_b200 import _lib as L
+    small = qk.make_contract(n_paths=10_000, n_steps=10)
+    for reserve, want in ((0, 2048), (-1, 0), (512, 512)):
+        free0 = torch.cuda.mem_get_info(0)[0]
+        with qk.Server(handle, 2048, 8, reserve_mib=reserve) as srv:
+            assert srv.stats()["reserved_mib"] == want
+            free_in = torch.cuda.mem_get_info(0)[0]
+            t = srv.submit(small)
+            while srv.poll(t, 1000) is None:
+                pass
+        free1 = torch.cuda.mem_get_info(0)[0]
+        assert free0 - free_in >= (want << 20) - (64 << 20)
+        assert abs(free1 - free0) < 256 << 20  # the reservation went back to the device
+    with pytest.raises(RuntimeError) as err:
+        qk.Server(handle, 2048, 8, reserve_mib=1 << 30)  # 1 PiB
+    assert err.value.status == L.QK_ERR_CAPACITY
+    with pytest.raises(ValueError):
+        qk.Server(handle, 2048, 8, reserve_mib=-2)
+
+
 def test_mixed_batch_sample_vs_closed_forms(qk, handle, oracle):
     """European legs of the seeded mixed batch within 3 SE (+ discretisation allowance for Euler)
     of the Gil-Pelaez price, priced together in one batch with all Greeks."""
