@@ -627,16 +627,23 @@ __global__ void __launch_bounds__(kLsmBlock, QK_LSM_MIN_BLOCKS) lsm_sweep_kernel
         if (c < n_chunks) issue(c, s, false, true);
         cp_async_commit();
     }
+    // With 4-byte rows every thread copies (issue) and later reads back exactly the
+    // same four paths of each array (elements 4t .. 4t+3 of a chunk), so its own
+    // cp.async.wait_group is all the ordering a chunk needs and a stage it refills
+    // holds only data it has itself consumed: no block barrier per chunk.  With
+    // 8-byte rows a thread reads slots that other threads copied.
+    constexpr bool kOwnSlots = kPer16 == 4;
+    static_assert(!kOwnSlots || kLsmChunk == 4 * kLsmBlock, "one 16-byte copy per thread and array");
+    if constexpr (kOwnSlots) __syncthreads();  // this date's coefficient stores visible
     // FP32 6-term kernel: the coefficients in registers, as pairs for the paired FMAs
     float2 cc[kF32 ? 6 : 1];
     if constexpr (kF32) {
-        __syncthreads();  // cuf stores visible
 #pragma unroll
         for (int i = 0; i < 6; ++i) cc[i] = make_float2(cuf[i], cuf[i]);
     }
     for (int k = 0; chunk < n_chunks; ++k, chunk += gridDim.x) {
         cp_async_wait_pending<ST - 2>();  // this thread's copies of `chunk` have landed
-        __syncthreads();  // ... and every other thread's; all threads are done with chunk k - 1
+        if constexpr (!kOwnSlots) __syncthreads();  // ... and every other thread's; all are done with chunk k - 1
         // refill the stage chunk k - 1 used, overlapping this chunk's arithmetic
         const int64_t ahead = chunk + static_cast<int64_t>(ST - 1) * gridDim.x;
         if (ahead < n_chunks) issue(ahead, (k + ST - 1) % ST, true, true);
