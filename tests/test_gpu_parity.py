@@ -430,6 +430,36 @@ def test_lane_modes_simulate_the_same_paths(qk, handle, model, scheme, lam):
         assert a["prob_itm"] == pytest.approx(b["prob_itm"], rel=1e-12, abs=1e-15)
 
 
+@pytest.mark.parametrize("model", [0, 1])
+def test_qe_near_zero_variance_lane_modes_and_fp64(qk, handle, model):
+    """QE with the Feller condition far from holding (vol-of-vol 0.9, long-run variance 0.01,
+    kappa 0.5): the variance sits near zero and a large share of steps leaves the quadratic
+    regime, often for one path of a lane's pair only.  Two paths per lane and one path per
+    lane still simulate bit-identical paths (prices agree to the rounding of the moment
+    merge), and the FP32 prices stay within one standard error of the FP64 engine on the same
+    draws (three combined SE under Bates, where the two precisions decide jumps from different
+    bits)."""
+    legs = [qk.payoff(qk.EUROPEAN, qk.PUT, 100.0), qk.payoff(qk.ASIAN, qk.CALL, 100.0),
+            qk.payoff(qk.BARRIER_DOWN_OUT, qk.PUT, 100.0, 80.0)]
+    base = dict(model=model, scheme=qk.ANDERSEN_QE, v0=0.01, theta=0.01, kappa=0.5, sigma=0.9, rho=-0.7,
+                lambda_j=0.2 if model else 0.0, mu_j=-0.05, sigma_j=0.1, n_paths=100_001, n_steps=126, T=0.5,
+                seed=21, payoffs=legs)
+    c = qk.make_contract(precision=qk.FP32, **base)
+    out = []
+    try:
+        for lanes in (1, 2):
+            handle.tune_set(qk.FP32, model, qk.ANDERSEN_QE, 24, False, lanes)
+            out.append(qk.price_batch([c], None, handle)[0]["legs"])
+    finally:
+        handle.tune_reset()
+    for a, b in zip(out[0], out[1]):
+        assert a["price"] == pytest.approx(b["price"], rel=1e-12, abs=1e-15)
+        assert a["std_error"] == pytest.approx(b["std_error"], rel=1e-9)
+    r64 = qk.price_batch([qk.make_contract(precision=qk.FP64, **base)], None, handle)[0]["legs"]
+    for a, b in zip(out[1], r64):
+        assert abs(a["price"] - b["price"]) < (1.0 if model == 0 else 3.0 * 2 ** 0.5) * b["std_error"], (a, b)
+
+
 def test_edge_sizes_match_oracle(qk, handle, oracle):
     """Ragged and minimal sizes: a single path, partial warps, a single step, an empty request
     list, and the largest path count a contract may have (32-bit Philox path counter)."""
