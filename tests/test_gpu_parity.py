@@ -20,8 +20,14 @@ pytestmark = pytest.mark.gpu
 
 
 def test_step_trace_matches_reference_golden(qk, handle):
+    """One step on fed draws against the reference's own FP64 and FP32 builds: FP64 within
+    1e-12; FP32 within 1e-5 of the reference's FP32 build.  Where the reference's two builds
+    themselves differ by more than 1e-5 (11 of the 600 cases: variance 0 to 1e-4 at a
+    vol-of-vol of 0.9, where FP32 rounding moves a QE step across a regime threshold), the
+    FP32 step must agree with one of the two builds."""
     cases = load("step_cases.json")
     worst = {0: 0.0, 1: 0.0}
+    n_boundary = 0
     for c in cases:
         k = case_contract(qk.make_contract, c)
         z = np.array([c["z"]])
@@ -32,10 +38,13 @@ def test_step_trace_matches_reference_golden(qk, handle):
                 e = step_err(S[0], v[0], c["S_out64"], c["v_out64"], c["v"])
                 assert e <= TOL_STEP_FP64, (c, e)
             else:
-                e = min(step_err(S[0], v[0], c["S_out32"], c["v_out32"], c["v"]),
-                        step_err(S[0], v[0], c["S_out64"], c["v_out64"], c["v"]))
+                e = step_err(S[0], v[0], c["S_out32"], c["v_out32"], c["v"])
+                if step_err(c["S_out32"], c["v_out32"], c["S_out64"], c["v_out64"], c["v"]) > TOL_STEP_FP32:
+                    n_boundary += 1
+                    e = min(e, step_err(S[0], v[0], c["S_out64"], c["v_out64"], c["v"]))
                 assert e <= TOL_STEP_FP32, (c, e)
             worst[prec] = max(worst[prec], e)
+    assert n_boundary == 11
     print("worst per-step error FP64 %.2e FP32 %.2e" % (worst[0], worst[1]))
 
 

@@ -46,9 +46,12 @@ def test_oracle_steps_match_reference(oracle, precision):
             e = step_err(S[0], v[0], c["S_out64"], c["v_out64"], c["v"])
             assert e <= TOL_STEP_FP64, (c, e)
         else:
-            # matches the reference FP32 build, or is within the tolerance of the FP64 result
-            e = min(step_err(S[0], v[0], c["S_out32"], c["v_out32"], c["v"]),
-                    step_err(S[0], v[0], c["S_out64"], c["v_out64"], c["v"]))
+            # within the tolerance of the reference FP32 build; where that build itself is
+            # further than the tolerance from the FP64 one (a regime threshold crossed by FP32
+            # rounding near zero variance), within the tolerance of either
+            e = step_err(S[0], v[0], c["S_out32"], c["v_out32"], c["v"])
+            if step_err(c["S_out32"], c["v_out32"], c["S_out64"], c["v_out64"], c["v"]) > TOL_STEP_FP32:
+                e = min(e, step_err(S[0], v[0], c["S_out64"], c["v_out64"], c["v"]))
             assert e <= TOL_STEP_FP32, (c, e)
         worst = max(worst, e)
     assert len(cases) >= 500
