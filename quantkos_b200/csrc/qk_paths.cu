@@ -231,42 +231,26 @@ __device__ __forceinline__ void simulate_path(const StepConst<R> &p, R S0, R v0,
 // a), path b with every normal negated and the same Poisson uniforms.  Otherwise
 // two independent paths, each with its own draws, interleaved for instruction-level
 // parallelism.
-template <class R, int MODEL, int SCHEME, bool NEG>
-__device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R> &a, PathState<R> &b, uint32_t wa1,
-                                             uint32_t wa2, uint32_t wb1, uint32_t wb2, uint32_t pois_a,
-                                             uint32_t pois_b, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path_a,
-                                             uint32_t path_b, uint32_t stream, int n) {
-    if constexpr (sizeof(R) == 4) {
-        // both paths' normals (paired Box-Muller unless b mirrors a), then one paired step
-        float2 Z1, Z2;
-        if constexpr (NEG) {
-            float za1, za2;
-            Math<float>::box_muller(wa1, wa2, za1, za2);
-            Z1 = make_float2(za1, -za1);
-            Z2 = make_float2(za2, -za2);
-        } else {
-            Math<float>::box_muller_two(wa1, wa2, wb1, wb2, Z1, Z2);
-        }
-        float2 S2 = make_float2(a.S, b.S), v2 = make_float2(a.v, b.v);
-        if constexpr (SCHEME == kQE) step_qe_two_f32(p, S2, v2, Z1, Z2);
-        else if constexpr (SCHEME == kMilstein) step_milstein_two_f32(p, S2, v2, Z1, Z2);
-        else step_euler_two_f32(p, S2, v2, Z1, Z2);
-        a.S = S2.x;
-        b.S = S2.y;
-        a.v = v2.x;
-        b.v = v2.y;
+// FP32 normals of one step of a lane's two paths: paired Box-Muller, or path b the
+// mirror of path a (antithetic pair).
+template <bool NEG>
+__device__ __forceinline__ void normals_two_f32(uint32_t wa1, uint32_t wa2, uint32_t wb1, uint32_t wb2, float2 &Z1,
+                                                float2 &Z2) {
+    if constexpr (NEG) {
+        float za1, za2;
+        Math<float>::box_muller(wa1, wa2, za1, za2);
+        Z1 = make_float2(za1, -za1);
+        Z2 = make_float2(za2, -za2);
     } else {
-        R za1, za2, zb1, zb2;
-        Math<R>::box_muller(wa1, wa2, za1, za2);
-        if constexpr (NEG) {
-            zb1 = -za1;
-            zb2 = -za2;
-        } else {
-            Math<R>::box_muller(wb1, wb2, zb1, zb2);
-        }
-        heston_step<R, SCHEME>(p, a.S, a.v, za1, za2);
-        heston_step<R, SCHEME>(p, b.S, b.v, zb1, zb2);
+        Math<float>::box_muller_two(wa1, wa2, wb1, wb2, Z1, Z2);
     }
+}
+
+// Bates jumps of both paths of a lane after their Heston step.
+template <class R, int MODEL, bool NEG>
+__device__ __forceinline__ void jumps_two(const StepConst<R> &p, PathState<R> &a, PathState<R> &b, uint32_t pois_a,
+                                          uint32_t pois_b, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path_a,
+                                          uint32_t path_b, uint32_t stream, int n) {
     if constexpr (MODEL == kBates) {
         uint32_t word;
         if constexpr (NEG) {
@@ -310,6 +294,48 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
     }
 }
 
+// One FP32 step of a lane's two paths from their normals (the paired scheme step, then
+// the jumps).
+template <int MODEL, int SCHEME, bool NEG>
+__device__ __forceinline__ void step_two_z_f32(const StepConst<float> &p, PathState<float> &a, PathState<float> &b,
+                                               float2 Z1, float2 Z2, uint32_t pois_a, uint32_t pois_b, uint32_t kmin,
+                                               uint32_t k0, uint32_t k1, uint32_t path_a, uint32_t path_b,
+                                               uint32_t stream, int n) {
+    float2 S2 = make_float2(a.S, b.S), v2 = make_float2(a.v, b.v);
+    if constexpr (SCHEME == kQE) step_qe_two_f32(p, S2, v2, Z1, Z2);
+    else if constexpr (SCHEME == kMilstein) step_milstein_two_f32(p, S2, v2, Z1, Z2);
+    else step_euler_two_f32(p, S2, v2, Z1, Z2);
+    a.S = S2.x;
+    b.S = S2.y;
+    a.v = v2.x;
+    b.v = v2.y;
+    jumps_two<float, MODEL, NEG>(p, a, b, pois_a, pois_b, kmin, k0, k1, path_a, path_b, stream, n);
+}
+
+template <class R, int MODEL, int SCHEME, bool NEG>
+__device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R> &a, PathState<R> &b, uint32_t wa1,
+                                             uint32_t wa2, uint32_t wb1, uint32_t wb2, uint32_t pois_a,
+                                             uint32_t pois_b, uint32_t kmin, uint32_t k0, uint32_t k1, uint32_t path_a,
+                                             uint32_t path_b, uint32_t stream, int n) {
+    if constexpr (sizeof(R) == 4) {
+        float2 Z1, Z2;
+        normals_two_f32<NEG>(wa1, wa2, wb1, wb2, Z1, Z2);
+        step_two_z_f32<MODEL, SCHEME, NEG>(p, a, b, Z1, Z2, pois_a, pois_b, kmin, k0, k1, path_a, path_b, stream, n);
+    } else {
+        R za1, za2, zb1, zb2;
+        Math<R>::box_muller(wa1, wa2, za1, za2);
+        if constexpr (NEG) {
+            zb1 = -za1;
+            zb2 = -za2;
+        } else {
+            Math<R>::box_muller(wb1, wb2, zb1, zb2);
+        }
+        heston_step<R, SCHEME>(p, a.S, a.v, za1, za2);
+        heston_step<R, SCHEME>(p, b.S, b.v, zb1, zb2);
+        jumps_two<R, MODEL, NEG>(p, a, b, pois_a, pois_b, kmin, k0, k1, path_a, path_b, stream, n);
+    }
+}
+
 template <class R, int MODEL, int SCHEME, bool NEG, bool TRK = true, class Gen, class Sink2>
 __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
                                              uint32_t k0, uint32_t k1, uint32_t path_a, uint32_t path_b,
@@ -340,6 +366,20 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
                 poisson_words<R>(wa, pa, n, qa0, qa1);
                 if constexpr (!NEG) poisson_words<R>(wb, pb, n, qb0, qb1);
             }
+            if constexpr (sizeof(R) == 4 && SCHEME != kQE) {
+                // Euler and Milstein: both steps' normals first, so that the second step's
+                // Box-Muller (independent of the first step) overlaps the first step's work
+                // (QE, whose step holds more live values, measures faster without it)
+                float2 Z1a, Z2a, Z1b, Z2b;
+                normals_two_f32<NEG>(wa.x, wa.y, wb.x, wb.y, Z1a, Z2a);
+                normals_two_f32<NEG>(wa.z, wa.w, wb.z, wb.w, Z1b, Z2b);
+                step_two_z_f32<MODEL, SCHEME, NEG>(p, a, b, Z1a, Z2a, qa0, qb0, kmin, k0, k1, path_a, path_b, stream, n);
+                if constexpr (TRK) track(a, blk_a);
+                if constexpr (TRK) track(b, blk_b);
+                sink(n, a.S, a.v, b.S, b.v);
+                step_two_z_f32<MODEL, SCHEME, NEG>(p, a, b, Z1b, Z2b, qa1, qb1, kmin, k0, k1, path_a, path_b, stream,
+                                                   n + 1);
+            } else {
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.x, wa.y, wb.x, wb.y, qa0, qb0, kmin, k0, k1, path_a,
                                                 path_b, stream, n);
             if constexpr (TRK) track(a, blk_a);
@@ -347,6 +387,7 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
             sink(n, a.S, a.v, b.S, b.v);
             one_step_two<R, MODEL, SCHEME, NEG>(p, a, b, wa.z, wa.w, wb.z, wb.w, qa1, qb1, kmin, k0, k1, path_a,
                                                 path_b, stream, n + 1);
+            }
             if constexpr (TRK) track(a, blk_a);
             if constexpr (TRK) track(b, blk_b);
             sink(n + 1, a.S, a.v, b.S, b.v);
