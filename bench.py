@@ -399,7 +399,7 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
            "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "contracts_per_s": st["contracts_per_s"],
            "path_steps_per_s": st["path_steps_per_s"], "offered_path_steps_per_s": offered / arrivals[-1],
            "batches": st["batches"], "rejected": st["rejected"], "busy_s": st["busy_s"],
-           "lanes": lanes or 4, "wave_ms": wave_ms or 10.0, "reserved_mib": reserved_mib,
+           "lanes": lanes or 4, "wave_ms": wave_ms or 2.5, "reserved_mib": reserved_mib,
            "warmup_requests": len(warm),
            "batch_all_contracts_per_s": n_requests / (t_all * 1e-3),
            "batch_all_path_steps_per_s": offered / (t_all * 1e-3),

@@ -377,7 +377,7 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
 /* The same with all options: lanes = host threads, each with its own handle and stream,
  * whose waves run on the GPU at the same time (0 = 4); wave_ms = estimated GPU time at
  * which a lane closes the wave it is admitting, raised to the lane's share of the
- * waiting requests' estimated time when that is larger (0 = 10 ms; a wave always takes
+ * waiting requests' estimated time when that is larger (0 = 2.5 ms; a wave always takes
  * at least one request); reserve_mib = HBM mapped into the device's memory pool at the
  * start and held until qk_serve_stop, from which the lanes' buffers grow (0 = the
  * budget; -1 = none; mapping new memory while lanes run blocks every lane's driver

@@ -103,7 +103,7 @@ struct qk_server {
     int device = 0;
     size_t budget = 0, in_use = 0;
     int max_batch = 256;
-    double wave_us = 10000.0;  // GPU-time budget of one wave (the least a wave is allowed to hold)
+    double wave_us = 2500.0;  // GPU-time budget of one wave (the least a wave is allowed to hold)
     double queued_us = 0.0;   // estimated GPU time of the requests waiting for admission
     int n_lanes = 1;
     size_t reserved = 0;  // bytes held in the device pool for the lanes (pool_reserve)
@@ -224,7 +224,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     if (!h || !opt || !out) return qk::fail(QK_ERR_INVALID_ARG, "NULL argument");
     *out = nullptr;
     if (opt->lanes < 0 || opt->lanes > 16) return qk::fail(QK_ERR_INVALID_ARG, "lanes must be in [0, 16] (0 = 4)");
-    if (opt->wave_ms < 0.0) return qk::fail(QK_ERR_INVALID_ARG, "wave_ms must be >= 0 (0 = 10 ms)");
+    if (opt->wave_ms < 0.0) return qk::fail(QK_ERR_INVALID_ARG, "wave_ms must be >= 0 (0 = 2.5 ms)");
     if (opt->reserve_mib < -1) return qk::fail(QK_ERR_INVALID_ARG, "reserve_mib must be >= -1 (0 = the budget, -1 = none)");
     const int64_t hbm_budget_mib = opt->hbm_budget_mib;
     const int32_t max_batch = opt->max_batch;
@@ -235,7 +235,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     s->device = h->device;
     s->budget = hbm_budget_mib > 0 ? static_cast<size_t>(hbm_budget_mib) << 20 : static_cast<size_t>(free_b * 0.8);
     s->max_batch = max_batch > 0 ? max_batch : 256;
-    s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 10000.0;
+    s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 2500.0;
     const int lanes = opt->lanes > 0 ? opt->lanes : 4;
     s->n_lanes = lanes;
     const size_t reserve = opt->reserve_mib > 0 ? static_cast<size_t>(opt->reserve_mib) << 20

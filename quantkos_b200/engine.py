@@ -363,7 +363,7 @@ class Server:
     def __init__(self, handle: Handle | None = None, hbm_budget_mib: int = 0, max_batch: int = 256, lanes: int = 0,
                  wave_ms: float = 0.0, reserve_mib: int = 0):
         """lanes: host threads whose waves run on the GPU at once (0 = 4); wave_ms: estimated GPU time at
-        which a lane closes a wave (0 = 10 ms); reserve_mib: HBM mapped into the device pool at the start and
+        which a lane closes a wave (0 = 2.5 ms); reserve_mib: HBM mapped into the device pool at the start and
         held until stop, from which the lanes' buffers grow (0 = the budget, -1 = none)."""
         self.handle = handle or default_handle()
         self._s = C.c_void_p()
