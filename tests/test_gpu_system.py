@@ -244,24 +244,34 @@ def test_server_records_account_for_every_request(qk, handle):
 def test_server_reserves_pool_memory(qk, handle):
     """The server maps its reservation into the device pool at the start (0 = the budget, -1 =
     none, else the MiB given), holds it while it runs and gives it back at the stop; an
-    explicit reservation that cannot fit fails with QK_ERR_CAPACITY and leaves nothing held."""
-    import torch
+    explicit reservation that cannot fit fails with QK_ERR_CAPACITY and leaves nothing held.
+    Read from the pool's own counters (memory it has mapped), since a reservation may reuse
+    blocks the pool already held."""
+    from cuda.bindings import runtime as rt
     from quantkos_b200 import _lib as L
+
+    def pool_reserved() -> int:
+        err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+        assert err == rt.cudaError_t.cudaSuccess
+        err, v = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent)
+        assert err == rt.cudaError_t.cudaSuccess
+        return int(v)
+
     small = qk.make_contract(n_paths=10_000, n_steps=10)
     for reserve, want in ((0, 2048), (-1, 0), (512, 512)):
-        free0 = torch.cuda.mem_get_info(0)[0]
+        r0 = pool_reserved()
         with qk.Server(handle, 2048, 8, reserve_mib=reserve) as srv:
             assert srv.stats()["reserved_mib"] == want
-            free_in = torch.cuda.mem_get_info(0)[0]
+            assert pool_reserved() >= want << 20
             t = srv.submit(small)
             while srv.poll(t, 1000) is None:
                 pass
-        free1 = torch.cuda.mem_get_info(0)[0]
-        assert free0 - free_in >= (want << 20) - (64 << 20)
-        assert abs(free1 - free0) < 256 << 20  # the reservation went back to the device
+        assert pool_reserved() <= r0 + (256 << 20)  # the reservation went back to the device
+    r0 = pool_reserved()
     with pytest.raises(RuntimeError) as err:
         qk.Server(handle, 2048, 8, reserve_mib=1 << 30)  # 1 PiB
     assert err.value.status == L.QK_ERR_CAPACITY
+    assert pool_reserved() <= r0 + (256 << 20)
     with pytest.raises(ValueError):
         qk.Server(handle, 2048, 8, reserve_mib=-2)
 
