@@ -93,7 +93,8 @@ def parse_args():
                     help="launch shape 'tiles_per_warp,guided_tail,paths_per_lane' instead of the autotuner")
     ap.add_argument("--paths", type=int, default=N_PATHS,
                     help="paths per contract (the workload uses 16,777,216; smaller only for profiling captures)")
-    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve", "kinds", "attribution"],
+    ap.add_argument("--workload", choices=["bates5", "plain", "lsm", "batch", "serve", "kinds", "attribution",
+                                           "published_asian"],
                     default="bates5",
                     help="bates5 (default): the headline line; the others measure the remaining workloads")
     ap.add_argument("--subset", type=int, default=128, help="batch: contracts priced by both engines")
@@ -501,6 +502,42 @@ def run_other_workload(args) -> None:
                     config={"workload": f"fp32_kernel_kinds_european_{N_PATHS}x{N_STEPS}", "kinds": kinds,
                             "sfu_ops_per_s": sfu_ops, "issue_lane_ops_per_s": issue_ops,
                             "algorithmic_ops": {"issue": ISSUE_OPS, "sfu": SFU_OPS}},
+                    gpu_launches=None)
+    elif args.workload == "published_asian":
+        # the reference's one published benchmark (benchmarks/configs/
+        # bench_asian_option_price_no_greeks.yaml): Heston QE, arithmetic Asian call,
+        # 5,000,000 paths x 365 steps; its parameters and published price come from the
+        # committed fixture of the reference's test values.  Timed like the headline:
+        # resident descriptors (graph replay) and end to end from host structs, FP32.
+        fx = json.loads((ROOT / "tests" / "golden" / "reference_tests.json").read_text())["asian_benchmark"]
+        pp = fx["params"]
+        c = qk.make_contract(S0=pp["S0"], v0=pp["v0"], r=pp["r"], q=pp["q"], scheme=qk.ANDERSEN_QE, kappa=pp["kappa"],
+                             theta=pp["theta"], sigma=pp["sigma"], rho=pp["rho"], T=pp["T"], n_steps=pp["n_steps"],
+                             n_paths=pp["n_paths"], seed=88471920573105, precision=qk.FP32,
+                             payoffs=[qk.payoff(qk.ASIAN, qk.CALL, pp["K"])])
+        tuned = [] if args.no_autotune else h.autotune([c], None, reps=1)
+        prep = qk.PreparedBatch([c], None, h)
+        for _ in range(max(args.warmup, 3)):
+            prep.run()
+            prep.fetch()
+        with sampler:
+            ts = _timed(torch, ext, lambda: (prep.run(), prep.fetch()), args.steps, flush)
+            te = _timed(torch, ext, lambda: qk.price_batch([c], None, h), args.steps, flush)
+        leg = qk.price_batch([c], None, h)[0]["legs"][0]
+        ps = float(pp["n_paths"]) * pp["n_steps"]
+        ms, ms_e = statistics.mean(ts), statistics.mean(te)
+        line.update(value=ps / (ms * 1e-3), ms_per_step=ms, dtype="f32",
+                    config={"workload": "published_asian_heston_qe_5000000x365_fp32", "price": leg["price"],
+                            "std_error": leg["std_error"], "published_price": fx["price"],
+                            "published_std_error": fx["std_error"],
+                            "diff_in_combined_se": (leg["price"] - fx["price"]) / math.hypot(leg["std_error"],
+                                                                                           fx["std_error"]),
+                            "contracts_per_s": 1e3 / ms, "e2e_ms": ms_e, "e2e_path_steps_per_s": ps / (ms_e * 1e-3),
+                            "autotune": _shape_summary(tuned),
+                            # the reference's published timings of this run (its README), other hardware
+                            "published_reference": {"path_steps_per_s": 1.870e10, "seconds": 0.0976,
+                                                    "build": "CUDA FP32 fast-math",
+                                                    "hardware": "RTX 3060 Laptop GPU (sm_86)"}},
                     gpu_launches=None)
     elif args.workload == "lsm":
         pk_file = ROOT / "MEASURED_PEAKS.json"
