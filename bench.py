@@ -18,9 +18,11 @@ reported.  Prints ONE JSON line on rank 0.
 
 At N = 1 the line also carries the other workloads, each with its own clock
 record: `batch_4096` (the 4096-contract mix with all seven Greeks, batched FP32
-engine against the plain FP64 drop-in on every contract) and `serve` /
+engine against the plain FP64 drop-in on every contract), `serve` /
 `serve_sub_capacity` (Poisson request streams at 2,000 and 1,000 requests/s, 30%
-American puts).  `--no-extra` leaves them out.
+American puts) and `serve_vs_plain` (one stream at 200 requests/s served by the
+batched engine and by the plain FP64 method behind the same server: latency at equal
+load).  `--no-extra` leaves them out.
 """
 from __future__ import annotations
 
@@ -102,6 +104,8 @@ def parse_args():
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--lanes", type=int, default=0, help="serve: server lanes (0 = the library default)")
     ap.add_argument("--wave-ms", type=float, default=0.0, help="serve: wave budget in ms (0 = the library default)")
+    ap.add_argument("--serve-plain", action="store_true",
+                    help="serve: price every request alone with the plain FP64 method behind the same server")
     ap.add_argument("--no-extra", action="store_true",
                     help="default line without the 4096-contract batch and serving records")
     ap.add_argument("--batch-compare", type=int, default=4096,
@@ -340,7 +344,7 @@ def measure_batch_mix(qk, W, h, torch, ext, flush, subset: int | None = None, au
 
 
 def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, plain_sample: int = 0,
-                    lanes: int = 0, wave_ms: float = 0.0) -> dict:
+                    lanes: int = 0, wave_ms: float = 0.0, plain_fp64: bool = False) -> dict:
     """A Poisson stream of `n_requests` pricing requests at `rate` per second (30% American
     puts by LSM) submitted in real time to the continuous-batching server started on h;
     latency is submit to completion.  Optionally the plain FP64 one-contract-per-launch
@@ -352,7 +356,7 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
     import threading
 
     arrivals, contracts = W.serving_stream(n_requests, rate_per_s=rate)
-    srv = qk.Server(h, 0, 512, lanes, wave_ms)
+    srv = qk.Server(h, 0, 512, lanes, wave_ms, plain_fp64=plain_fp64)
     # warm the server that is measured: its lanes' device arenas grow to the sizes the
     # stream's largest requests need (one at a time, so every lane takes some), untimed;
     # the statistics below cover the stream's own tickets only
@@ -396,6 +400,7 @@ def measure_serving(qk, W, h, torch, ext, flush, rate: float, n_requests: int, p
     qk.price_batch(contracts[:64], None, h)
     t_all = _timed(torch, ext, lambda: qk.price_batch(contracts, None, h), 1, flush)[0]
     rec = {"workload": f"serving_{n_requests}_requests_poisson_{rate:g}_per_s_30pct_american",
+           "method": "plain_fp64_one_contract_per_launch" if plain_fp64 else "batched_fp32_engine",
            "rate_per_s": rate, "requests": n_requests, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
            "p999_ms": st["p999_ms"], "max_ms": st["max_ms"], "contracts_per_s": st["contracts_per_s"],
            "path_steps_per_s": st["path_steps_per_s"], "offered_path_steps_per_s": offered / arrivals[-1],
@@ -622,7 +627,8 @@ def run_other_workload(args) -> None:
         _, contracts = W.serving_stream(256)
         tuned = [] if args.no_autotune else h.autotune(contracts[:256], None, reps=1)
         rec = measure_serving(qk, W, h, torch, ext, flush, rate=args.rate, n_requests=args.requests,
-                              plain_sample=args.subset, lanes=args.lanes, wave_ms=args.wave_ms)
+                              plain_sample=args.subset, lanes=args.lanes, wave_ms=args.wave_ms,
+                              plain_fp64=args.serve_plain)
         rec["autotune"] = _shape_summary(tuned)
         line.update(metric="contracts/s", unit="contracts/s", value=rec["contracts_per_s"], dtype="f32",
                     ms_per_step=None, config=rec, gpu_launches=None)
@@ -853,6 +859,14 @@ def main() -> None:
             line["serve"] = measure_serving(qk, W, h, torch, ext, flush, rate=2000.0, n_requests=20_000)
             line["serve_sub_capacity"] = measure_serving(qk, W, h, torch, ext, flush, rate=1000.0,
                                                          n_requests=10_000)
+            # both methods behind the same server on one stream, at a rate the plain FP64
+            # method sustains: latency at equal load
+            keys = ("p50_ms", "p99_ms", "p999_ms", "max_ms", "contracts_per_s", "clocks")
+            vs = {}
+            for name, plain in (("batched", False), ("plain_fp64", True)):
+                r = measure_serving(qk, W, h, torch, ext, flush, rate=200.0, n_requests=3_000, plain_fp64=plain)
+                vs[name] = {k: r[k] for k in keys}
+            line["serve_vs_plain"] = {"workload": "serving_3000_requests_poisson_200_per_s_30pct_american", **vs}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

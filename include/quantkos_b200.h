@@ -383,14 +383,19 @@ qk_status qk_serve_start(qk_handle *h, int64_t hbm_budget_mib, int32_t max_batch
  * budget; -1 = none; mapping new memory while lanes run blocks every lane's driver
  * calls for up to hundreds of milliseconds).  A default reservation that does not fit
  * is skipped; an explicit one that does not fit fails with QK_ERR_CAPACITY.
- * hbm_budget_mib and max_batch as above.  qk_serve_start uses the defaults for lanes,
- * wave_ms and reserve_mib. */
+ * hbm_budget_mib and max_batch as above.  plain_fp64 = 1 serves every request alone
+ * with the plain FP64 method (qk_price_plain: one contract, all FP64, one launch per
+ * pricing task) behind the same lanes and admission, for comparing the two methods on
+ * one request stream; 0 = the batched engine.  qk_serve_start uses the defaults for
+ * lanes, wave_ms, reserve_mib and plain_fp64. */
 typedef struct qk_serve_options {
     int64_t hbm_budget_mib;
     int32_t max_batch;
     int32_t lanes;
     double wave_ms;
     int64_t reserve_mib;
+    int32_t plain_fp64;
+    int32_t pad_;
 } qk_serve_options;
 qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server **out);
 qk_status qk_serve_submit(qk_server *s, const qk_contract *c, const qk_greeks *g, int64_t *ticket);

@@ -127,7 +127,7 @@ class ServeRecord(C.Structure):
 
 class ServeOptions(C.Structure):
     _fields_ = [("hbm_budget_mib", C.c_int64), ("max_batch", C.c_int32), ("lanes", C.c_int32), ("wave_ms", C.c_double),
-                ("reserve_mib", C.c_int64)]
+                ("reserve_mib", C.c_int64), ("plain_fp64", C.c_int32), ("pad_", C.c_int32)]
 
 
 _P = C.POINTER

@@ -107,6 +107,7 @@ struct qk_server {
     double queued_us = 0.0;   // estimated GPU time of the requests waiting for admission
     int n_lanes = 1;
     size_t reserved = 0;  // bytes held in the device pool for the lanes (pool_reserve)
+    bool plain = false;   // one request per wave, priced by the plain FP64 method
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request> queue;
@@ -145,7 +146,8 @@ static void lane_loop(qk_server *s, qk_handle *h, int lane) {
                 // (small waves while the queue is short, large ones under load)
                 const double cap = std::max(s->wave_us, s->queued_us / s->n_lanes);
                 est = 0.0;
-                while (!s->queue.empty() && static_cast<int>(batch.size()) < s->max_batch &&
+                const int wave_max = s->plain ? 1 : s->max_batch;
+                while (!s->queue.empty() && static_cast<int>(batch.size()) < wave_max &&
                        s->in_use + bytes + s->queue.front().bytes <= s->budget &&
                        (batch.empty() || est + s->queue.front().est_us <= cap)) {
                     bytes += s->queue.front().bytes;
@@ -169,7 +171,8 @@ static void lane_loop(qk_server *s, qk_handle *h, int lane) {
             gs[i] = batch[i].g;
         }
         const auto t0 = Clock::now();
-        const qk_status st = qk::price_contracts(h, cs.data(), static_cast<int32_t>(cs.size()), gs.data(), rs.data(), false);
+        const qk_status st =
+            qk::price_contracts(h, cs.data(), static_cast<int32_t>(cs.size()), gs.data(), rs.data(), s->plain);
         const auto t1 = Clock::now();
         {
             std::lock_guard<std::mutex> lk(s->mu);
@@ -236,6 +239,7 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
     s->budget = hbm_budget_mib > 0 ? static_cast<size_t>(hbm_budget_mib) << 20 : static_cast<size_t>(free_b * 0.8);
     s->max_batch = max_batch > 0 ? max_batch : 256;
     s->wave_us = opt->wave_ms > 0.0 ? opt->wave_ms * 1e3 : 2500.0;
+    s->plain = opt->plain_fp64 != 0;
     const int lanes = opt->lanes > 0 ? opt->lanes : 4;
     s->n_lanes = lanes;
     const size_t reserve = opt->reserve_mib > 0 ? static_cast<size_t>(opt->reserve_mib) << 20

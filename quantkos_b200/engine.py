@@ -361,13 +361,14 @@ class Server:
     """Continuous-batching request loop (qk_serve_*)."""
 
     def __init__(self, handle: Handle | None = None, hbm_budget_mib: int = 0, max_batch: int = 256, lanes: int = 0,
-                 wave_ms: float = 0.0, reserve_mib: int = 0):
+                 wave_ms: float = 0.0, reserve_mib: int = 0, plain_fp64: bool = False):
         """lanes: host threads whose waves run on the GPU at once (0 = 4); wave_ms: estimated GPU time at
         which a lane closes a wave (0 = 2.5 ms); reserve_mib: HBM mapped into the device pool at the start and
-        held until stop, from which the lanes' buffers grow (0 = the budget, -1 = none)."""
+        held until stop, from which the lanes' buffers grow (0 = the budget, -1 = none); plain_fp64: serve
+        every request alone with the plain FP64 method (for comparing the methods on one stream)."""
         self.handle = handle or default_handle()
         self._s = C.c_void_p()
-        opt = L.ServeOptions(hbm_budget_mib, max_batch, lanes, wave_ms, reserve_mib)
+        opt = L.ServeOptions(hbm_budget_mib, max_batch, lanes, wave_ms, reserve_mib, int(bool(plain_fp64)), 0)
         check(L.lib().qk_serve_start_ex(self.handle.ptr, C.byref(opt), C.byref(self._s)), "qk_serve_start_ex")
 
     def submit(self, contract: L.Contract, greeks: L.Greeks | None = None) -> int:

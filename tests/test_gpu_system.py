@@ -241,6 +241,29 @@ def test_server_records_account_for_every_request(qk, handle):
     assert st["p50_ms"] == lat[int(0.5 * (len(lat) - 1) + 0.5)]
 
 
+def test_server_plain_fp64_mode_equals_price_plain(qk, handle):
+    """plain_fp64 = 1: every request is priced alone by the plain FP64 method behind the same
+    lanes; each result equals qk_price_plain on that contract bit for bit, one wave per request."""
+    from quantkos_b200 import workloads as W
+    _, contracts = W.serving_stream(24, seed=17)
+    for c in contracts:
+        c.n_paths = min(c.n_paths, 40_000)
+    with qk.Server(handle, 4096, 16, lanes=2, reserve_mib=-1, plain_fp64=True) as srv:
+        tickets = [srv.submit(c) for c in contracts]
+        got = []
+        for tk in tickets:
+            r = None
+            while r is None:
+                r = srv.poll(tk, 1000)
+            got.append(r)
+        recs = srv.records()
+    assert all(r["wave_requests"] == 1 for r in recs) and len(recs) == len(contracts)
+    for c, g in zip(contracts, got):
+        want = qk.price_plain(c, None, handle)
+        for a, b in zip(g["legs"], want["legs"]):
+            assert a["price"] == b["price"] and a["std_error"] == b["std_error"]
+
+
 def test_server_reserves_pool_memory(qk, handle):
     """The server maps its reservation into the device pool at the start (0 = the budget, -1 =
     none, else the MiB given), holds it while it runs and gives it back at the stop; an
