@@ -246,10 +246,13 @@ qk_status qk_serve_start_ex(qk_handle *h, const qk_serve_options *opt, qk_server
                            : opt->reserve_mib == 0 ? s->budget : 0;
     if (reserve > 0) {
         const qk_status st = qk::pool_reserve(h->device, h->stream, reserve);
-        if (st == QK_OK) s->reserved = reserve;
-        else if (opt->reserve_mib > 0) {
+        if (st == QK_OK) {
+            s->reserved = reserve;
+        } else if (opt->reserve_mib > 0) {
             delete s;
             return st;
+        } else {
+            qk::g_last_error.clear();  // a default reservation that does not fit is skipped, not an error
         }
     }
     for (int i = 0; i < lanes; ++i) {
