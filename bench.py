@@ -574,6 +574,15 @@ def run_other_workload(args) -> None:
                               "sweep_ms": t["reduce_ms"], "forward_ms": t["device_ms"] - t["reduce_ms"]},
                     gpu_launches=args.steps * t["launches"])
         line["roofline"]["frac"] = line["roofline"]["achieved"] / line["roofline"]["peak"]
+        # the forward kernel (Heston QE paths, FP32, writing the 50 exercise-date slabs):
+        # SFU-bound like the path kernels, 12 SFU operations per path-step
+        sfu_ops = h.measure_sfu()
+        fwd_ms = line["roofline"]["forward_ms"]
+        line["forward"] = {"kernel": "slab_paths_two_kernel<float, Heston, QE>", "ms": fwd_ms,
+                           "path_steps_per_s": ps / (fwd_ms * 1e-3), "bound": "sfu",
+                           "frac_of_sfu_bound": ps / (fwd_ms * 1e-3) / (sfu_ops / SFU_PER_STEP),
+                           "slab_bytes_written": 8.0 * c32.n_paths * 50,
+                           "slab_write_gbs": 8.0 * c32.n_paths * 50 / (fwd_ms * 1e-3) / 1e9}
     elif args.workload == "attribution":
         # Where the 4096-contract mix loses against its kinds' standalone rates: the mix
         # timed whole; each kernel kind's share of the mix (its contracts, all Greeks)
