@@ -336,14 +336,19 @@ __device__ __forceinline__ void one_step_two(const StepConst<R> &p, PathState<R>
     }
 }
 
+// ssum_slot: where the two paths' Asian running sums (x: path a, y: path b) are kept
+// between the 16-step blocks that add to them: this thread's shared-memory slot (two
+// FP64 sums read and written once per block, four registers fewer in the step loop),
+// or nullptr for a.ssum and b.ssum.
 template <class R, int MODEL, int SCHEME, bool NEG, bool TRK = true, class Gen, class Sink2>
 __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, int n_steps, const Gen &gen,
                                              uint32_t k0, uint32_t k1, uint32_t path_a, uint32_t path_b,
                                              uint32_t stream, uint32_t kmin, PathState<R> &a, PathState<R> &b,
-                                             Sink2 &&sink) {
+                                             Sink2 &&sink, double2 *ssum_slot = nullptr) {
     a.S = b.S = S0;
     a.v = b.v = v0;
     a.ssum = b.ssum = 0.0;
+    if (TRK && ssum_slot) *ssum_slot = make_double2(0.0, 0.0);
     a.smax = b.smax = S0;
     a.smin = b.smin = S0;
     for (int n0 = 0; n0 < n_steps; n0 += kSumChunk) {
@@ -414,9 +419,20 @@ __device__ __forceinline__ void simulate_two(const StepConst<R> &p, R S0, R v0, 
             sink(n, a.S, a.v, b.S, b.v);
         }
         if constexpr (TRK) {
-            a.ssum += static_cast<double>(blk_a);
-            b.ssum += static_cast<double>(blk_b);
+            if (ssum_slot) {
+                double2 s = *ssum_slot;
+                s.x += static_cast<double>(blk_a);
+                s.y += static_cast<double>(blk_b);
+                *ssum_slot = s;
+            } else {
+                a.ssum += static_cast<double>(blk_a);
+                b.ssum += static_cast<double>(blk_b);
+            }
         }
+    }
+    if (TRK && ssum_slot) {
+        a.ssum = ssum_slot->x;
+        b.ssum = ssum_slot->y;
     }
 }
 
@@ -477,6 +493,8 @@ __global__ void __launch_bounds__(path_block_max<R>(),
     // task), keeps the tile's running moments per leg in its own shared-memory slots and
     // writes one record per leg.  No block-wide barrier anywhere.
     __shared__ Moments s_acc[path_block_max<R>() / 32][QK_MAX_PAYOFFS];
+    // the two-path lanes' Asian running sums (simulate_two); one slot per thread
+    __shared__ double2 s_ssum[(LANE != kLaneOne && TRK) ? path_block_max<R>() : 1];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);  // OptionPricer.hpp:316
@@ -523,10 +541,10 @@ __global__ void __launch_bounds__(path_block_max<R>(),
                 if (active) {
                     if constexpr (UK) {
                         simulate_two<R, MODEL, SCHEME, NEG, TRK>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1, pa, pb, stream,
-                                                            kmin, sa, sb, NoSink2{});
+                                                            kmin, sa, sb, NoSink2{}, &s_ssum[threadIdx.x]);
                     } else {
                         simulate_two<R, MODEL, SCHEME, NEG, TRK>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1, pa, pb,
-                                                            stream, kmin, sa, sb, NoSink2{});
+                                                            stream, kmin, sa, sb, NoSink2{}, &s_ssum[threadIdx.x]);
                     }
                 } else {
                     sa.S = sa.smax = sa.smin = sb.S = sb.smax = sb.smin = R(0);
