@@ -493,8 +493,10 @@ __global__ void __launch_bounds__(path_block_max<R>(),
     // task), keeps the tile's running moments per leg in its own shared-memory slots and
     // writes one record per leg.  No block-wide barrier anywhere.
     __shared__ Moments s_acc[path_block_max<R>() / 32][QK_MAX_PAYOFFS];
-    // the two-path lanes' Asian running sums (simulate_two); one slot per thread
-    __shared__ double2 s_ssum[(LANE != kLaneOne && TRK) ? path_block_max<R>() : 1];
+    // the Asian running sums of a lane's two independent paths (simulate_two); one slot per
+    // thread (antithetic pairs keep theirs in registers, which measures faster there)
+    constexpr bool kSumSlot = LANE == kLaneTwo && TRK;
+    __shared__ double2 s_ssum[kSumSlot ? path_block_max<R>() : 1];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const R eps_payoff = sizeof(R) == 4 ? R(1e-6) : R(1e-12);  // OptionPricer.hpp:316
@@ -541,10 +543,10 @@ __global__ void __launch_bounds__(path_block_max<R>(),
                 if (active) {
                     if constexpr (UK) {
                         simulate_two<R, MODEL, SCHEME, NEG, TRK>(p, S0, v0, n_steps, ParamKeys{rk}, k0, k1, pa, pb, stream,
-                                                            kmin, sa, sb, NoSink2{}, &s_ssum[threadIdx.x]);
+                                                            kmin, sa, sb, NoSink2{}, kSumSlot ? &s_ssum[threadIdx.x] : nullptr);
                     } else {
                         simulate_two<R, MODEL, SCHEME, NEG, TRK>(p, S0, v0, n_steps, RegKeys{k0, k1}, k0, k1, pa, pb,
-                                                            stream, kmin, sa, sb, NoSink2{}, &s_ssum[threadIdx.x]);
+                                                            stream, kmin, sa, sb, NoSink2{}, kSumSlot ? &s_ssum[threadIdx.x] : nullptr);
                     }
                 } else {
                     sa.S = sa.smax = sa.smin = sb.S = sb.smax = sb.smin = R(0);
