@@ -76,14 +76,15 @@ constexpr int kKindStreams = 8;
 }  // namespace qk
 
 // Launch shape of each kernel kind, [precision (FP64, FP32)][model][scheme], that a
-// handle starts with: in FP32 48 tiles per warp slot and two paths per lane, with the
-// guided tail except for Heston QE (the shapes measured fastest on large contracts;
-// qk_autotune picks per workload); in FP64 24 tiles and one path per lane.
+// handle starts with: in FP32 48 tiles per warp slot, two paths per lane and blocks of
+// 512 threads, with the guided tail except for Heston QE (the shapes measured fastest
+// on large contracts; qk_autotune picks per workload); in FP64 24 tiles, one path per
+// lane and blocks of 256 threads.
 using ShapeTable = std::array<std::array<std::array<int, 3>, 2>, 2>;
 constexpr ShapeTable kDefaultTilesPerWarp = {{{{{{24, 24, 24}}, {{24, 24, 24}}}}, {{{{48, 48, 48}}, {{48, 48, 48}}}}}};
 constexpr ShapeTable kDefaultGuidedTail = {{{{{{0, 0, 0}}, {{0, 0, 0}}}}, {{{{1, 1, 0}}, {{1, 1, 1}}}}}};
 constexpr ShapeTable kDefaultPathsPerLane = {{{{{{1, 1, 1}}, {{1, 1, 1}}}}, {{{{2, 2, 2}}, {{2, 2, 2}}}}}};
-constexpr ShapeTable kDefaultBlock = {{{{{{256, 256, 256}}, {{256, 256, 256}}}}, {{{{256, 256, 256}}, {{256, 256, 256}}}}}};
+constexpr ShapeTable kDefaultBlock = {{{{{{256, 256, 256}}, {{256, 256, 256}}}}, {{{{512, 512, 512}}, {{512, 512, 512}}}}}};
 
 struct qk_handle {
     int device = 0;
