@@ -353,7 +353,7 @@ void DevArena::release() {
 qk_status HostArena::ensure(size_t bytes) {
     if (bytes <= cap) return QK_OK;
     const size_t want = std::max<size_t>({bytes, cap + cap / 2, size_t(1) << 20});
-    if (ptr) cudaFreeHost(ptr);
+    if (ptr) retired.push_back(ptr);  // freed by release(): no device-wide synchronization here
     ptr = nullptr;
     cap = 0;
     QK_CUDA_TRY(cudaMallocHost(&ptr, want));
@@ -362,6 +362,8 @@ qk_status HostArena::ensure(size_t bytes) {
 }
 void HostArena::release() {
     if (ptr) cudaFreeHost(ptr);
+    for (void *r : retired) cudaFreeHost(r);
+    retired.clear();
     ptr = nullptr;
     cap = 0;
 }

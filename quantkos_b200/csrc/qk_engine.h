@@ -30,6 +30,11 @@ struct DevArena {
 struct HostArena {
     void *ptr = nullptr;
     size_t cap = 0;
+    // Buffers outgrown while the handle lives: cudaFreeHost synchronizes the whole
+    // device, so a growth keeps the old buffer here and release() (at handle
+    // destruction, after its stream has drained) frees them all.  Geometric growth
+    // keeps their total below the current buffer's size.
+    std::vector<void *> retired;
     qk_status ensure(size_t bytes);
     void release();
 };
